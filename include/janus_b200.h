@@ -1,0 +1,177 @@
+/*
+ * janus_b200 — C ABI of the B200-native Lippmann–Schwinger hot path.
+ *
+ * Plain C types only: device pointers are `void*` / typed pointers into GPU
+ * memory the caller owns, streams are `cudaStream_t` passed as `void*`
+ * (NULL = legacy default stream), shapes are `int64_t` arrays.  Every entry
+ * point returns an `int` status: JB_OK (0) on success, a negative JB_E*
+ * code on failure, with a message in jb_last_error() (per calling thread).
+ * No exception crosses this boundary.  Host wrappers map JB_EINVAL to
+ * ValueError and every other code to RuntimeError, like the reference's
+ * checkarray/green validation (janus/utils/checkarray.pyx:3-53,
+ * janus/green.pyx:102-109, 146-161).
+ *
+ * Conventions (those of the reference): fields are row-major
+ * `T[n0][n1][(n2)][s]` with the Mandel component fastest, s = 3 (2D) or 6
+ * (3D), Mandel order (xx, yy, xy) / (xx, yy, zz, √2 yz, √2 zx, √2 xy).
+ * Spectra are `T[n0][(n1)][n_last/2+1][2]` (real/imaginary interleaved along
+ * the last axis, the reference's FFT output layout).  A "batch" L of fields
+ * is L such arrays back to back.  T is double (JB_F64) or float (JB_F32).
+ *
+ * Each entry point below names the reference interface it replaces.
+ */
+#ifndef JANUS_B200_H
+#define JANUS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define JB_OK 0
+#define JB_EINVAL (-1)   /* invalid argument (shape, size, range) */
+#define JB_ECUDA (-2)    /* CUDA runtime error */
+#define JB_ENOMEM (-3)   /* device allocation failed */
+#define JB_ESTATE (-4)   /* call not valid in the handle's state */
+
+#define JB_F64 0
+#define JB_F32 1
+
+#define JB_TRUNCATED 0
+#define JB_FILTERED 1
+
+typedef struct jb_fft_s jb_fft;
+typedef struct jb_green_s jb_green;
+typedef struct jb_local_s jb_local;
+typedef struct jb_solver_s jb_solver;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int jb_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char *jb_last_error(void);
+/* Largest supported length of one grid axis for a precision. */
+int jb_max_axis_length(int dtype);
+
+/* ---- real FFT objects ------------------------------------------------- */
+
+/* Replaces janus.fft.serial.create_real (janus/fft/serial/_serial_fft.pyx:
+ * 20-53) and the _RealFFT2D/_RealFFT3D constructors (55-74, 179-200).
+ * `flags` is accepted for interface parity (FFTW planner flags, 10-18). */
+int jb_fft_create(int dim, const int64_t *shape, int dtype, unsigned flags,
+                  jb_fft **out);
+int jb_fft_destroy(jb_fft *fft);
+/* _RealFFT2D/3D.r2c (152-163, 296-309): unnormalised forward transform.
+ * r: real T[n0][n1][(n2)] with element strides r_strides (dim entries,
+ * in elements, may be NULL for C-contiguous); c: T[oshape] contiguous. */
+int jb_fft_r2c(jb_fft *fft, const void *r, const int64_t *r_strides, void *c,
+               void *stream);
+/* _RealFFT2D/3D.c2r (165-177, 311-325): inverse transform scaled by 1/N.
+ * c is not modified. */
+int jb_fft_c2r(jb_fft *fft, const void *c, void *r, const int64_t *r_strides,
+               void *stream);
+
+/* ---- continuous Green operator (host, per wave-vector) ---------------- */
+
+/* _GreenOperatorForStrains2D/3D.c_set_frequency + c_to_memoryview
+ * (janus/material/elastic/linear/isotropic.pyx:158-206, 227-353): the
+ * s x s Mandel matrix of Gamma0(k) for shear modulus g, Poisson ratio nu,
+ * row-major into out. Same operations as the reference. */
+int jb_green_continuous_matrix(int dim, double g, double nu, const double *k,
+                               double *out);
+/* _GreenOperatorForStrains2D/3D.c_apply (isotropic.pyx:186-193, 294-313):
+ * y = Gamma0(k) x for one s-vector, host, reference operation order. */
+int jb_green_continuous_apply(int dim, double g, double nu, const double *k,
+                              const double *x, double *y);
+/* FourthRankIsotropicTensor2D/3D.c_apply (janus/operators.pyx:317-324,
+ * 354-365): y = (sph J + dev K) x for one s-vector, host, reference
+ * operation order; x == y allowed. */
+int jb_isotropic_apply(int dim, double sph, double dev, const double *x,
+                       double *y);
+
+/* ---- discrete Green operators ----------------------------------------- */
+
+/* Replaces janus.green.truncated / filtered (janus/green.pyx:22-36) and the
+ * TruncatedGreenOperator2D/3D, FilteredGreenOperator2D/3D constructors
+ * (100-141, 261-307, 428-430, 501-503, 593-605, 708-728). */
+int jb_green_create(int dim, const int64_t *shape, double h, double g,
+                    double nu, int variant, int dtype, jb_green **out);
+int jb_green_destroy(jb_green *green);
+/* DiscreteGreenOperator2D/3D.c_apply and the fused truncated loops
+ * (green.pyx:185-216, 356-390, 456-495, 534-580): y = Gamma0[x] for a batch
+ * of `batch` contiguous fields; x == y is allowed. */
+int jb_green_apply(jb_green *green, const void *x, void *y, int64_t batch,
+                   void *stream);
+/* set_frequency + to_memoryview at index b (green.pyx:146-171, 312-342 and
+ * the subclasses' c_set_frequency / c_to_memoryview): host, FP64, with the
+ * reference's range checks (0 <= b_i < n_i). */
+int jb_green_matrix(jb_green *green, const int32_t *b, double *out);
+/* apply_by_freq (green.pyx:173-180, 344-351): eta = Gamma(b) tau, host. */
+int jb_green_apply_by_freq(jb_green *green, const int32_t *b,
+                           const double *tau, double *eta);
+/* Device form of apply_by_freq over `count` indices: b int32[count][dim],
+ * tau/eta complex T[count][s][2] (may alias). Uses the same spectral
+ * contraction as jb_green_apply. */
+int jb_green_apply_by_freq_device(jb_green *green, int64_t count,
+                                  const int32_t *b, const void *tau,
+                                  void *eta, void *stream);
+
+/* ---- local operators (C - C0):eps ------------------------------------- */
+
+/* Replaces BlockDiagonalOperator2D/3D built from FourthRankIsotropicTensor
+ * local operators (janus/operators.pyx:617-716, 257-408): phase-map form.
+ * sph/dev: host arrays of nphase coefficients; phase: device array of
+ * n0*n1*(n2) indices, uint8 (index_bytes 1) or int32 (4), copied. */
+int jb_local_create(int dim, const int64_t *shape, int nphase,
+                    const double *sph, const double *dev, const void *phase,
+                    int index_bytes, int dtype, jb_local **out);
+int jb_local_destroy(jb_local *local);
+/* BlockDiagonalOperator2D/3D.c_apply (657-664, 708-716), bitwise the
+ * reference arithmetic; x == y allowed. */
+int jb_local_apply(jb_local *local, const void *x, void *y, int64_t batch,
+                   void *stream);
+/* BlockDiagonalLinearOperator2D/3D.c_apply / c_apply_transpose (739-774,
+ * 823-861): y[v] = a[v] x[v] (or a[v]^T x[v]); a: T[nvox][osz][isz]. */
+int jb_block_linear_apply(int dtype, int64_t nvox, int osz, int isz,
+                          const void *a, const void *x, void *y,
+                          int transpose, void *stream);
+
+/* ---- basic fixed-point scheme ----------------------------------------- */
+
+/* The loop of sphinx/tutorials/square_basic/square_basic.py:83-97 over
+ * `nload` load cases at once: eps_{k+1} = E - Gamma0[(C - C0):eps_k],
+ * res_k = ||eps_{k+1} - eps_k|| / (sqrt(N) ||E||). */
+int jb_solver_create(jb_green *green, jb_local *local, int nload,
+                     jb_solver **out);
+int jb_solver_destroy(jb_solver *solver);
+/* eps: device T[nload][grid][s]; E: host double[nload][s]. If init != 0,
+ * eps is set to E first.  Runs until every load case has res <= tol or
+ * max_iter iterations.  residuals: host double[max_iter][nload] (may be
+ * NULL); iters_out: iterations done; mean_tau: host double[nload][s], the
+ * grid mean of (C - C0):eps at the final eps (may be NULL).  The call
+ * returns after the work on `stream` has completed. */
+int jb_solver_run(jb_solver *solver, const double *E, void *eps, int init,
+                  int max_iter, double tol, double *residuals, int *iters_out,
+                  double *mean_tau, void *stream);
+/* Set the macroscopic strains E (host double[nload][s]) used by
+ * jb_solver_step. */
+int jb_solver_set_load(jb_solver *solver, const double *E);
+/* One iteration on `stream`, asynchronous: eps is updated in place and the
+ * normalised residual of each load case is written to res_dev (device
+ * double[nload], may be NULL). */
+int jb_solver_step(jb_solver *solver, void *eps, double *res_dev,
+                   void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JANUS_B200_H */

@@ -1,0 +1,109 @@
+"""ctypes binding of the janus_b200 C ABI (``include/janus_b200.h``).
+
+The native library ``janus_b200/lib/libjanus_b200.so`` is the only compute
+path: there is no CPU fallback.  If the library is missing it is built with
+nvcc (``janus_b200.build``); if that fails, importing any operator raises.
+Status codes map to exceptions like the reference's validation layer:
+JB_EINVAL -> ValueError, anything else -> RuntimeError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from . import build as _build
+
+JB_OK = 0
+JB_EINVAL = -1
+JB_F64 = 0
+JB_F32 = 1
+JB_TRUNCATED = 0
+JB_FILTERED = 1
+
+_lock = threading.Lock()
+_lib = None
+
+c_void_p = ctypes.c_void_p
+c_int = ctypes.c_int
+c_int64 = ctypes.c_int64
+c_double = ctypes.c_double
+P_int64 = ctypes.POINTER(ctypes.c_int64)
+P_int32 = ctypes.POINTER(ctypes.c_int32)
+P_double = ctypes.POINTER(ctypes.c_double)
+P_int = ctypes.POINTER(ctypes.c_int)
+
+_SIGS = {
+    "jb_version": ([], c_int),
+    "jb_last_error": ([], ctypes.c_char_p),
+    "jb_max_axis_length": ([c_int], c_int),
+    "jb_fft_create": ([c_int, P_int64, c_int, ctypes.c_uint, ctypes.POINTER(c_void_p)], c_int),
+    "jb_fft_destroy": ([c_void_p], c_int),
+    "jb_fft_r2c": ([c_void_p, c_void_p, P_int64, c_void_p, c_void_p], c_int),
+    "jb_fft_c2r": ([c_void_p, c_void_p, c_void_p, P_int64, c_void_p], c_int),
+    "jb_green_continuous_matrix": ([c_int, c_double, c_double, P_double, P_double], c_int),
+    "jb_green_continuous_apply": ([c_int, c_double, c_double, P_double, P_double, P_double],
+                                  c_int),
+    "jb_isotropic_apply": ([c_int, c_double, c_double, P_double, P_double], c_int),
+    "jb_green_create": ([c_int, P_int64, c_double, c_double, c_double, c_int, c_int,
+                         ctypes.POINTER(c_void_p)], c_int),
+    "jb_green_destroy": ([c_void_p], c_int),
+    "jb_green_apply": ([c_void_p, c_void_p, c_void_p, c_int64, c_void_p], c_int),
+    "jb_green_matrix": ([c_void_p, P_int32, P_double], c_int),
+    "jb_green_apply_by_freq": ([c_void_p, P_int32, P_double, P_double], c_int),
+    "jb_green_apply_by_freq_device": ([c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                       c_void_p], c_int),
+    "jb_local_create": ([c_int, P_int64, c_int, P_double, P_double, c_void_p, c_int, c_int,
+                         ctypes.POINTER(c_void_p)], c_int),
+    "jb_local_destroy": ([c_void_p], c_int),
+    "jb_local_apply": ([c_void_p, c_void_p, c_void_p, c_int64, c_void_p], c_int),
+    "jb_block_linear_apply": ([c_int, c_int64, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                               c_int, c_void_p], c_int),
+    "jb_solver_create": ([c_void_p, c_void_p, c_int, ctypes.POINTER(c_void_p)], c_int),
+    "jb_solver_destroy": ([c_void_p], c_int),
+    "jb_solver_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_double, P_double, P_int,
+                       P_double, c_void_p], c_int),
+    "jb_solver_set_load": ([c_void_p, P_double], c_int),
+    "jb_solver_step": ([c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+}
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def lib():
+    """Load (building first if needed) the native library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            path = _build.LIB
+            if not os.path.exists(path):
+                _build.build()
+            handle = ctypes.CDLL(path)
+            for name, (args, res) in _SIGS.items():
+                fn = getattr(handle, name)
+                fn.argtypes = args
+                fn.restype = res
+            _lib = handle
+    return _lib
+
+
+def check(status: int) -> None:
+    if status == JB_OK:
+        return
+    msg = lib().jb_last_error().decode(errors="replace")
+    if status == JB_EINVAL:
+        raise ValueError(msg)
+    raise RuntimeError(f"janus_b200 native call failed ({status}): {msg}")
+
+
+def i64_array(values):
+    arr = (c_int64 * len(values))(*[int(v) for v in values])
+    return arr
+
+
+def f64_array(values):
+    return (c_double * len(values))(*[float(v) for v in values])

@@ -1,0 +1,915 @@
+// C ABI of janus_b200 (declared in include/janus_b200.h): handle objects,
+// argument validation with the reference's error semantics, host-side
+// per-wave-vector Green matrices, and the orchestration of the pass kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/janus_b200.h"
+#include "jb_kernels.h"
+
+using jb::AxisData;
+using jb::F32;
+using jb::F64;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define JB_CUDA(expr)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? JB_ENOMEM : JB_ECUDA,                \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define JB_TRY(expr)          \
+  do {                        \
+    int r_ = (expr);          \
+    if (r_ != JB_OK) return r_; \
+  } while (0)
+
+size_t real_size(int dtype) { return dtype == F64 ? 8 : 4; }
+
+// radices used on the device: 8, 4, 2 for powers of two, then 3, 5, then
+// any remaining prime handled by the generic butterfly
+void factorize(int n, jb::AxisPlan& p) {
+  p.n = n;
+  p.nf = 0;
+  int m = n;
+  while (m % 8 == 0) { p.fac[p.nf++] = 8; m /= 8; }
+  while (m % 4 == 0) { p.fac[p.nf++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.fac[p.nf++] = 2; m /= 2; }
+  while (m % 3 == 0) { p.fac[p.nf++] = 3; m /= 3; }
+  while (m % 5 == 0) { p.fac[p.nf++] = 5; m /= 5; }
+  for (int f = 7; m > 1 && (long)f * f <= m; f += 2)
+    while (m % f == 0) { p.fac[p.nf++] = f; m /= f; }
+  if (m > 1) p.fac[p.nf++] = m;
+}
+
+struct DeviceBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+int dev_alloc(void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? JB_ENOMEM : JB_ECUDA,
+                std::string("cudaMalloc(") + std::to_string(bytes) +
+                    " bytes): " + cudaGetErrorString(e));
+  }
+  return JB_OK;
+}
+
+int ensure_buf(DeviceBuf& b, size_t bytes) {
+  if (b.bytes >= bytes && b.p) return JB_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  JB_TRY(dev_alloc(&b.p, bytes));
+  b.bytes = bytes;
+  return JB_OK;
+}
+
+// twiddle table exp(-2 pi i t / n) computed in long double, rounded once
+int make_axis(int n, int dtype, AxisData& ax) {
+  factorize(n, ax.plan);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  if (dtype == F64) {
+    std::vector<double> h(2 * (size_t)n);
+    for (int t = 0; t < n; ++t) {
+      long double a = two_pi * (long double)t / (long double)n;
+      h[2 * t] = (double)cosl(a);
+      h[2 * t + 1] = (double)-sinl(a);
+    }
+    JB_TRY(dev_alloc(&ax.tw, h.size() * sizeof(double)));
+    JB_CUDA(cudaMemcpy(ax.tw, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> h(2 * (size_t)n);
+    for (int t = 0; t < n; ++t) {
+      long double a = two_pi * (long double)t / (long double)n;
+      h[2 * t] = (float)cosl(a);
+      h[2 * t + 1] = (float)-sinl(a);
+    }
+    JB_TRY(dev_alloc(&ax.tw, h.size() * sizeof(float)));
+    JB_CUDA(cudaMemcpy(ax.tw, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return JB_OK;
+}
+
+int check_shape(int dim, const int64_t* shape, int dtype) {
+  if (dim != 2 && dim != 3)
+    return fail(JB_EINVAL, "length of shape must be 2 or 3 (was " + std::to_string(dim) + ")");
+  if (!shape) return fail(JB_EINVAL, "shape must not be NULL");
+  if (dtype != F64 && dtype != F32)
+    return fail(JB_EINVAL, "dtype must be JB_F64 or JB_F32");
+  for (int d = 0; d < dim; ++d) {
+    if (shape[d] <= 0)
+      return fail(JB_EINVAL, "shape" + std::to_string(d) + " should be > 0 (was " +
+                                 std::to_string(shape[d]) + ")");
+    if (shape[d] > jb::max_axis_length(dtype))
+      return fail(JB_EINVAL, "axis " + std::to_string(d) + " of length " +
+                                 std::to_string(shape[d]) + " exceeds the supported maximum " +
+                                 std::to_string(jb::max_axis_length(dtype)));
+  }
+  return JB_OK;
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+int launch_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return JB_OK;
+  if (e == cudaErrorInvalidValue)
+    return fail(JB_EINVAL, std::string(what) + ": unsupported size for the tiled kernels");
+  return fail(JB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// continuous Green operator, isotropic.pyx:158-182 / 227-290, same operations
+// ---------------------------------------------------------------------------
+struct GreenAux {
+  double d1, d2, d3, d4;
+};
+
+GreenAux green_aux(double g, double nu) {
+  // isotropic.pyx:135-138
+  return {1.0 / g, 0.5 / (g * (1.0 - nu)), 0.25 / g, 0.5 / g};
+}
+
+void green_matrix2(const GreenAux& a, const double* k, double* out) {
+  const double k0 = k[0], k1 = k[1];
+  double k0k0 = k0 * k0, k1k1 = k1 * k1;
+  double g00, g01, g02, g11, g12, g22;
+  if (k0k0 + k1k1 == 0.) {
+    g00 = g01 = g02 = g11 = g12 = g22 = 0.;
+  } else {
+    const double s = 1.0 / (k0k0 + k1k1);
+    k0k0 *= s;
+    k1k1 *= s;
+    const double k0k1 = s * k0 * k1;
+    g00 = k0k0 * (a.d1 - a.d2 * k0k0);
+    g11 = k1k1 * (a.d1 - a.d2 * k1k1);
+    const double dummy = -a.d2 * k0k0 * k1k1;
+    g01 = dummy;
+    g22 = 2 * (a.d3 + dummy);
+    g02 = M_SQRT2 * k0k1 * (a.d4 - a.d2 * k0k0);
+    g12 = M_SQRT2 * k0k1 * (a.d4 - a.d2 * k1k1);
+  }
+  const double m[9] = {g00, g01, g02, g01, g11, g12, g02, g12, g22};
+  std::memcpy(out, m, sizeof(m));
+}
+
+void green_matrix3(const GreenAux& a, const double* k, double* out) {
+  const double k0 = k[0], k1 = k[1], k2 = k[2];
+  double k0k0 = k0 * k0, k1k1 = k1 * k1, k2k2 = k2 * k2;
+  double g[6][6];
+  if (k0k0 + k1k1 + k2k2 == 0.) {
+    std::memset(out, 0, 36 * sizeof(double));
+    return;
+  }
+  const double s = 1.0 / (k0k0 + k1k1 + k2k2);
+  k0k0 *= s;
+  k1k1 *= s;
+  k2k2 *= s;
+  const double k1k2 = s * k1 * k2, k2k0 = s * k2 * k0, k0k1 = s * k0 * k1;
+  const double d1 = a.d1, d2 = a.d2, d3 = a.d3, d4 = a.d4;
+  g[0][0] = k0k0 * (d1 - d2 * k0k0);
+  g[1][1] = k1k1 * (d1 - d2 * k1k1);
+  g[2][2] = k2k2 * (d1 - d2 * k2k2);
+  g[3][3] = 2. * (d3 * (k1k1 + k2k2) - d2 * k1k1 * k2k2);
+  g[4][4] = 2. * (d3 * (k2k2 + k0k0) - d2 * k2k2 * k0k0);
+  g[5][5] = 2. * (d3 * (k0k0 + k1k1) - d2 * k0k0 * k1k1);
+  g[0][1] = -d2 * k0k0 * k1k1;
+  g[0][2] = -d2 * k0k0 * k2k2;
+  g[0][3] = -M_SQRT2 * d2 * k0k0 * k1k2;
+  g[0][4] = M_SQRT2 * k2k0 * (d4 - d2 * k0k0);
+  g[0][5] = M_SQRT2 * k0k1 * (d4 - d2 * k0k0);
+  g[1][2] = -d2 * k1k1 * k2k2;
+  g[1][3] = M_SQRT2 * k1k2 * (d4 - d2 * k1k1);
+  g[1][4] = -M_SQRT2 * d2 * k1k1 * k2k0;
+  g[1][5] = M_SQRT2 * k0k1 * (d4 - d2 * k1k1);
+  g[2][3] = M_SQRT2 * k1k2 * (d4 - d2 * k2k2);
+  g[2][4] = M_SQRT2 * k2k0 * (d4 - d2 * k2k2);
+  g[2][5] = -M_SQRT2 * d2 * k2k2 * k0k1;
+  g[3][4] = 2 * k0k1 * (d3 - d2 * k2k2);
+  g[3][5] = 2 * k2k0 * (d3 - d2 * k1k1);
+  g[4][5] = 2 * k1k2 * (d3 - d2 * k0k0);
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) {
+      out[i * 6 + j] = g[i][j];
+      out[j * 6 + i] = g[i][j];
+    }
+}
+
+void green_matrix_dim(int dim, const GreenAux& a, const double* k, double* out) {
+  if (dim == 2)
+    green_matrix2(a, k, out);
+  else
+    green_matrix3(a, k, out);
+}
+
+}  // namespace
+
+// ===========================================================================
+// handles
+// ===========================================================================
+
+struct jb_fft_s {
+  int dim = 0, dtype = 0;
+  int64_t n[3] = {1, 1, 1};
+  AxisData ax[3];
+  DeviceBuf scratch;
+};
+
+struct jb_green_s {
+  int dim = 0, dtype = 0, variant = 0;
+  int64_t n[3] = {1, 1, 1};
+  double h = 1, g = 1, nu = 0;
+  double s[3] = {0, 0, 0};
+  AxisData ax[3];
+  jb::GreenDeviceTables gt;
+  std::vector<void*> tables;
+  DeviceBuf spec;
+  DeviceBuf bidx;
+};
+
+struct jb_local_s {
+  int dim = 0, dtype = 0, nphase = 0, index_bytes = 1;
+  int64_t n[3] = {1, 1, 1};
+  int64_t nvox = 0;
+  void* phase = nullptr;
+  void* table = nullptr;
+};
+
+struct jb_solver_s {
+  jb_green* green = nullptr;
+  jb_local* local = nullptr;
+  int L = 1;
+  DeviceBuf spec, partials, E, res, mean, normd;
+  std::vector<double> Eh;
+  std::vector<double> norm;  // 1 / (sqrt(N) |E_l|)
+  int nb_rows = 0;
+  bool load_set = false;
+};
+
+namespace {
+
+void free_axes(AxisData* ax) {
+  for (int d = 0; d < 3; ++d)
+    if (ax[d].tw) {
+      cudaFree(ax[d].tw);
+      ax[d].tw = nullptr;
+    }
+}
+
+int upload_table(jb_green* g, int dtype, const std::vector<double>& v, void** out) {
+  void* p = nullptr;
+  const size_t rs = real_size(dtype);
+  JB_TRY(dev_alloc(&p, v.size() * rs));
+  g->tables.push_back(p);
+  if (dtype == F64) {
+    JB_CUDA(cudaMemcpy(p, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(v.begin(), v.end());
+    JB_CUDA(cudaMemcpy(p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+  }
+  *out = p;
+  return JB_OK;
+}
+
+// spectral passes shared by jb_green_apply and the solver
+// x: real fields (or eps with local), spec: complex scratch, y: output
+int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
+                 const jb::LocalDesc* local, const jb::UpdateDesc* upd, int* nb_rows,
+                 cudaStream_t st) {
+  const int dim = g->dim;
+  const int C = dim == 2 ? 3 : 6;
+  const int64_t n0 = g->n[0], n1 = g->n[1], n2 = g->n[2];
+  const int64_t nlast = dim == 2 ? n1 : n2;
+  const int64_t m = nlast / 2 + 1;
+  const int64_t N = dim == 2 ? n0 * n1 : n0 * n1 * n2;
+  jb::RealGeom geom{};
+  geom.cs = 1;
+  geom.es = C;
+  geom.ls = N * C;
+  if (dim == 2) {
+    geom.rows = n0;
+    geom.n1r = 1;
+    geom.s0 = n1 * C;
+    geom.s1 = 0;
+  } else {
+    geom.rows = n0 * n1;
+    geom.n1r = n1;
+    geom.s0 = n1 * n2 * C;
+    geom.s1 = n2 * C;
+  }
+  const AxisData& last = g->ax[dim - 1];
+  if ((int64_t)L > 65535) return fail(JB_EINVAL, "batch too large (max 65535)");
+  JB_TRY(launch_status(jb::launch_rows_r2c(g->dtype, last, C, (int)L, x, geom, spec, local, st),
+                       "rows_r2c"));
+  if (dim == 3)
+    JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 0, L * n0, m * C, spec, spec, C,
+                                         dim, nullptr, n1, m, st),
+                         "cols_fwd_axis1"));
+  const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
+  JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
+                                       &g->gt, n1, m, st),
+                       "cols_green_axis0"));
+  if (dim == 3)
+    JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 1, L * n0, m * C, spec, spec, C,
+                                         dim, nullptr, n1, m, st),
+                         "cols_inv_axis1"));
+  JB_TRY(launch_status(jb::launch_rows_c2r(g->dtype, last, C, (int)L, spec, y, geom,
+                                           1.0 / (double)N, upd, nb_rows, st),
+                       "rows_c2r"));
+  return JB_OK;
+}
+
+int64_t spec_elems(const jb_green* g) {
+  const int C = g->dim == 2 ? 3 : 6;
+  const int64_t nlast = g->dim == 2 ? g->n[1] : g->n[2];
+  const int64_t m = nlast / 2 + 1;
+  return (g->dim == 2 ? g->n[0] : g->n[0] * g->n[1]) * m * C;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jb_version(void) { return 100; }
+
+const char* jb_last_error(void) { return g_err.c_str(); }
+
+int jb_max_axis_length(int dtype) { return jb::max_axis_length(dtype); }
+
+// ---------------------------------------------------------------------------
+// FFT
+// ---------------------------------------------------------------------------
+
+int jb_fft_create(int dim, const int64_t* shape, int dtype, unsigned flags, jb_fft** out) {
+  (void)flags;
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  JB_TRY(check_shape(dim, shape, dtype));
+  jb_fft* f = new jb_fft();
+  f->dim = dim;
+  f->dtype = dtype;
+  for (int d = 0; d < dim; ++d) f->n[d] = shape[d];
+  for (int d = 0; d < dim; ++d) {
+    int r = make_axis((int)shape[d], dtype, f->ax[d]);
+    if (r != JB_OK) {
+      free_axes(f->ax);
+      delete f;
+      return r;
+    }
+  }
+  *out = f;
+  return JB_OK;
+}
+
+int jb_fft_destroy(jb_fft* f) {
+  if (!f) return JB_OK;
+  free_axes(f->ax);
+  if (f->scratch.p) cudaFree(f->scratch.p);
+  delete f;
+  return JB_OK;
+}
+
+static jb::RealGeom fft_geom(const jb_fft* f, const int64_t* strides) {
+  jb::RealGeom g{};
+  g.cs = 0;
+  g.ls = 0;
+  if (f->dim == 2) {
+    g.rows = f->n[0];
+    g.n1r = 1;
+    g.s0 = strides ? strides[0] : f->n[1];
+    g.s1 = 0;
+    g.es = strides ? strides[1] : 1;
+  } else {
+    g.rows = f->n[0] * f->n[1];
+    g.n1r = f->n[1];
+    g.s0 = strides ? strides[0] : f->n[1] * f->n[2];
+    g.s1 = strides ? strides[1] : f->n[2];
+    g.es = strides ? strides[2] : 1;
+  }
+  return g;
+}
+
+int jb_fft_r2c(jb_fft* f, const void* r, const int64_t* r_strides, void* c, void* stream) {
+  if (!f || !r || !c) return fail(JB_EINVAL, "NULL argument");
+  cudaStream_t st = as_stream(stream);
+  const jb::RealGeom g = fft_geom(f, r_strides);
+  const int dim = f->dim;
+  const int64_t nlast = f->n[dim - 1];
+  const int64_t m = nlast / 2 + 1;
+  JB_TRY(launch_status(jb::launch_rows_r2c(f->dtype, f->ax[dim - 1], 1, 1, r, g, c, nullptr, st),
+                       "fft rows_r2c"));
+  if (dim == 3)
+    JB_TRY(launch_status(jb::launch_cols(f->dtype, f->ax[1], 0, f->n[0], m, c, c, 1, dim,
+                                         nullptr, f->n[1], m, st),
+                         "fft cols axis1"));
+  const int64_t inner0 = dim == 2 ? m : f->n[1] * m;
+  JB_TRY(launch_status(
+      jb::launch_cols(f->dtype, f->ax[0], 0, 1, inner0, c, c, 1, dim, nullptr, f->n[1], m, st),
+      "fft cols axis0"));
+  return JB_OK;
+}
+
+int jb_fft_c2r(jb_fft* f, const void* c, void* r, const int64_t* r_strides, void* stream) {
+  if (!f || !r || !c) return fail(JB_EINVAL, "NULL argument");
+  cudaStream_t st = as_stream(stream);
+  const int dim = f->dim;
+  const int64_t nlast = f->n[dim - 1];
+  const int64_t m = nlast / 2 + 1;
+  const int64_t rows = dim == 2 ? f->n[0] : f->n[0] * f->n[1];
+  const size_t bytes = (size_t)rows * m * 2 * real_size(f->dtype);
+  JB_TRY(ensure_buf(f->scratch, bytes));
+  void* s = f->scratch.p;
+  const int64_t inner0 = dim == 2 ? m : f->n[1] * m;
+  JB_TRY(launch_status(
+      jb::launch_cols(f->dtype, f->ax[0], 1, 1, inner0, c, s, 1, dim, nullptr, f->n[1], m, st),
+      "fft cols axis0"));
+  if (dim == 3)
+    JB_TRY(launch_status(jb::launch_cols(f->dtype, f->ax[1], 1, f->n[0], m, s, s, 1, dim,
+                                         nullptr, f->n[1], m, st),
+                         "fft cols axis1"));
+  const jb::RealGeom g = fft_geom(f, r_strides);
+  double N = 1;
+  for (int d = 0; d < dim; ++d) N *= (double)f->n[d];
+  JB_TRY(launch_status(jb::launch_rows_c2r(f->dtype, f->ax[dim - 1], 1, 1, s, r, g, 1.0 / N,
+                                           nullptr, nullptr, st),
+                       "fft rows_c2r"));
+  return JB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// continuous Green operator
+// ---------------------------------------------------------------------------
+
+int jb_green_continuous_matrix(int dim, double g, double nu, const double* k, double* out) {
+  if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
+  if (!k || !out) return fail(JB_EINVAL, "NULL argument");
+  green_matrix_dim(dim, green_aux(g, nu), k, out);
+  return JB_OK;
+}
+
+int jb_green_continuous_apply(int dim, double g, double nu, const double* k, const double* x,
+                              double* y) {
+  if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
+  if (!k || !x || !y) return fail(JB_EINVAL, "NULL argument");
+  double m[36];
+  green_matrix_dim(dim, green_aux(g, nu), k, m);
+  const int S = dim == 2 ? 3 : 6;
+  double xv[6];
+  for (int i = 0; i < S; ++i) xv[i] = x[i];
+  for (int i = 0; i < S; ++i) {
+    double s = m[i * S] * xv[0];
+    for (int j = 1; j < S; ++j) s = s + m[i * S + j] * xv[j];
+    y[i] = s;
+  }
+  return JB_OK;
+}
+
+int jb_isotropic_apply(int dim, double sph, double dev, const double* x, double* y) {
+  if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
+  if (!x || !y) return fail(JB_EINVAL, "NULL argument");
+  const double tr = (sph - dev) / (double)dim;  // operators.pyx:299
+  if (dim == 2) {
+    const double x0 = x[0], x1 = x[1], x2 = x[2];
+    const double aux = tr * (x0 + x1);
+    y[0] = aux + dev * x0;
+    y[1] = aux + dev * x1;
+    y[2] = dev * x2;
+  } else {
+    const double x0 = x[0], x1 = x[1], x2 = x[2], x3 = x[3], x4 = x[4], x5 = x[5];
+    const double aux = tr * (x0 + x1 + x2);
+    y[0] = aux + dev * x0;
+    y[1] = aux + dev * x1;
+    y[2] = aux + dev * x2;
+    y[3] = dev * x3;
+    y[4] = dev * x4;
+    y[5] = dev * x5;
+  }
+  return JB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// discrete Green operators
+// ---------------------------------------------------------------------------
+
+int jb_green_create(int dim, const int64_t* shape, double h, double g, double nu, int variant,
+                    int dtype, jb_green** out) {
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  JB_TRY(check_shape(dim, shape, dtype));
+  if (!(h > 0.)) return fail(JB_EINVAL, "h must be > 0 (was " + std::to_string(h) + ")");
+  if (variant != JB_TRUNCATED && variant != JB_FILTERED)
+    return fail(JB_EINVAL, "variant must be JB_TRUNCATED or JB_FILTERED");
+  jb_green* G = new jb_green();
+  G->dim = dim;
+  G->dtype = dtype;
+  G->variant = variant;
+  G->h = h;
+  G->g = g;
+  G->nu = nu;
+  for (int d = 0; d < dim; ++d) {
+    G->n[d] = shape[d];
+    // green.pyx:140-141, 305-307
+    G->s[d] = 2. * M_PI / (h * (double)shape[d]);
+  }
+  auto cleanup = [&](int r) {
+    free_axes(G->ax);
+    for (void* p : G->tables) cudaFree(p);
+    delete G;
+    return r;
+  };
+  for (int d = 0; d < dim; ++d) {
+    int r = make_axis((int)shape[d], dtype, G->ax[d]);
+    if (r != JB_OK) return cleanup(r);
+  }
+  G->gt.variant = variant;
+  G->gt.inv2g = 0.5 / g;
+  G->gt.c1 = 1.0 / (1.0 - nu);
+  for (int d = 0; d < dim; ++d) {
+    const int64_t n = shape[d];
+    const double sd = G->s[d];
+    if (variant == JB_TRUNCATED) {
+      std::vector<double> kt(n);
+      for (int64_t b = 0; b < n; ++b) kt[b] = 2 * b > n ? sd * (b - n) : sd * b;
+      int r = upload_table(G, dtype, kt, &G->gt.kt[d]);
+      if (r != JB_OK) return cleanup(r);
+    } else {
+      std::vector<double> kn(n), kp(n), wn(n), wp(n);
+      for (int64_t b = 0; b < n; ++b) {
+        // green.pyx:616-648 / 738-808
+        double k = sd * (b - n);
+        double w = cos(0.25 * h * k);
+        w *= w;
+        kn[b] = k;
+        wn[b] = w;
+        k = sd * b;
+        w = cos(0.25 * h * k);
+        w *= w;
+        kp[b] = k;
+        wp[b] = w;
+      }
+      int r = upload_table(G, dtype, kn, &G->gt.kn[d]);
+      if (r == JB_OK) r = upload_table(G, dtype, kp, &G->gt.kp[d]);
+      if (r == JB_OK) r = upload_table(G, dtype, wn, &G->gt.wn[d]);
+      if (r == JB_OK) r = upload_table(G, dtype, wp, &G->gt.wp[d]);
+      if (r != JB_OK) return cleanup(r);
+    }
+  }
+  *out = G;
+  return JB_OK;
+}
+
+int jb_green_destroy(jb_green* G) {
+  if (!G) return JB_OK;
+  free_axes(G->ax);
+  for (void* p : G->tables) cudaFree(p);
+  if (G->spec.p) cudaFree(G->spec.p);
+  if (G->bidx.p) cudaFree(G->bidx.p);
+  delete G;
+  return JB_OK;
+}
+
+int jb_green_apply(jb_green* G, const void* x, void* y, int64_t batch, void* stream) {
+  if (!G || !x || !y) return fail(JB_EINVAL, "NULL argument");
+  if (batch < 1) return fail(JB_EINVAL, "batch must be >= 1");
+  const size_t bytes = (size_t)batch * spec_elems(G) * 2 * real_size(G->dtype);
+  JB_TRY(ensure_buf(G->spec, bytes));
+  return green_passes(G, x, y, batch, G->spec.p, nullptr, nullptr, nullptr,
+                      as_stream(stream));
+}
+
+static int check_b(const jb_green* G, const int32_t* b) {
+  if (!b) return fail(JB_EINVAL, "b must not be NULL");
+  for (int d = 0; d < G->dim; ++d)
+    if (b[d] < 0 || b[d] >= G->n[d])
+      return fail(JB_EINVAL, "index must be >= 0 and < " + std::to_string(G->n[d]) +
+                                 " (was " + std::to_string(b[d]) + ")");
+  return JB_OK;
+}
+
+int jb_green_matrix(jb_green* G, const int32_t* b, double* out) {
+  if (!G || !out) return fail(JB_EINVAL, "NULL argument");
+  JB_TRY(check_b(G, b));
+  const int dim = G->dim;
+  const int S = dim == 2 ? 3 : 6;
+  const GreenAux aux = green_aux(G->g, G->nu);
+  if (G->variant == JB_TRUNCATED) {
+    double k[3];
+    for (int d = 0; d < dim; ++d) {
+      const int64_t n = G->n[d];
+      k[d] = 2 * (int64_t)b[d] > n ? G->s[d] * (b[d] - n) : G->s[d] * b[d];
+    }
+    green_matrix_dim(dim, aux, k, out);
+    return JB_OK;
+  }
+  // filtered: aliases in the reference's order (all negative first, last
+  // axis fastest), weights multiplied axis by axis, terms summed left to
+  // right (green.pyx:609-670, 732-910)
+  double kk[3][2], ww[3][2];
+  for (int d = 0; d < dim; ++d) {
+    const int64_t n = G->n[d];
+    double k = G->s[d] * (b[d] - n);
+    double w = cos(0.25 * G->h * k);
+    w *= w;
+    kk[d][0] = k;
+    ww[d][0] = w;
+    k = G->s[d] * b[d];
+    w = cos(0.25 * G->h * k);
+    w *= w;
+    kk[d][1] = k;
+    ww[d][1] = w;
+  }
+  double acc[36], term[36];
+  const int na = 1 << dim;
+  for (int a = 0; a < na; ++a) {
+    double k[3];
+    double w = 1.0;
+    for (int d = 0; d < dim; ++d) {
+      const int c = (a >> (dim - 1 - d)) & 1;
+      k[d] = kk[d][c];
+      w = d == 0 ? ww[d][c] : w * ww[d][c];
+    }
+    green_matrix_dim(dim, aux, k, term);
+    for (int i = 0; i < S * S; ++i) acc[i] = a == 0 ? w * term[i] : acc[i] + w * term[i];
+  }
+  std::memcpy(out, acc, sizeof(double) * S * S);
+  return JB_OK;
+}
+
+int jb_green_apply_by_freq(jb_green* G, const int32_t* b, const double* tau, double* eta) {
+  if (!G || !tau || !eta) return fail(JB_EINVAL, "NULL argument");
+  double m[36];
+  JB_TRY(jb_green_matrix(G, b, m));
+  const int S = G->dim == 2 ? 3 : 6;
+  double x[6];
+  for (int i = 0; i < S; ++i) x[i] = tau[i];
+  for (int i = 0; i < S; ++i) {
+    // row i of the symmetric matrix times x, summed left to right like the
+    // reference's explicit expressions (isotropic.pyx:186-193, 294-313)
+    double s = m[i * S] * x[0];
+    for (int j = 1; j < S; ++j) s = s + m[i * S + j] * x[j];
+    eta[i] = s;
+  }
+  return JB_OK;
+}
+
+int jb_green_apply_by_freq_device(jb_green* G, int64_t count, const int32_t* b, const void* tau,
+                                  void* eta, void* stream) {
+  if (!G || !b || !tau || !eta) return fail(JB_EINVAL, "NULL argument");
+  if (count < 0) return fail(JB_EINVAL, "count must be >= 0");
+  if (count == 0) return JB_OK;
+  return launch_status(jb::launch_green_by_freq(G->dtype, G->dim, G->gt, count, b, tau, eta,
+                                                as_stream(stream)),
+                       "green_by_freq");
+}
+
+// ---------------------------------------------------------------------------
+// local operators
+// ---------------------------------------------------------------------------
+
+int jb_local_create(int dim, const int64_t* shape, int nphase, const double* sph,
+                    const double* dev, const void* phase, int index_bytes, int dtype,
+                    jb_local** out) {
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
+  if (dtype != F64 && dtype != F32) return fail(JB_EINVAL, "dtype must be JB_F64 or JB_F32");
+  if (nphase < 1) return fail(JB_EINVAL, "nphase must be >= 1");
+  if (index_bytes != 1 && index_bytes != 4) return fail(JB_EINVAL, "index_bytes must be 1 or 4");
+  if (index_bytes == 1 && nphase > 256) return fail(JB_EINVAL, "uint8 phase map allows 256 phases");
+  if (!sph || !dev || !phase) return fail(JB_EINVAL, "NULL argument");
+  jb_local* L = new jb_local();
+  L->dim = dim;
+  L->dtype = dtype;
+  L->nphase = nphase;
+  L->index_bytes = index_bytes;
+  L->nvox = 1;
+  for (int d = 0; d < dim; ++d) {
+    if (shape[d] <= 0) {
+      delete L;
+      return fail(JB_EINVAL, "shape must be > 0");
+    }
+    L->n[d] = shape[d];
+    L->nvox *= shape[d];
+  }
+  std::vector<double> tab(2 * (size_t)nphase);
+  for (int p = 0; p < nphase; ++p) {
+    tab[2 * p] = (sph[p] - dev[p]) / (double)dim;  // operators.pyx:299
+    tab[2 * p + 1] = dev[p];
+  }
+  const size_t rs = real_size(dtype);
+  int r = dev_alloc(&L->table, tab.size() * rs);
+  if (r == JB_OK) r = dev_alloc(&L->phase, (size_t)L->nvox * index_bytes);
+  if (r != JB_OK) {
+    if (L->table) cudaFree(L->table);
+    delete L;
+    return r;
+  }
+  cudaError_t e;
+  if (dtype == F64) {
+    e = cudaMemcpy(L->table, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice);
+  } else {
+    std::vector<float> f(tab.begin(), tab.end());
+    e = cudaMemcpy(L->table, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpy(L->phase, phase, (size_t)L->nvox * index_bytes, cudaMemcpyDefault);
+  if (e != cudaSuccess) {
+    cudaFree(L->table);
+    cudaFree(L->phase);
+    delete L;
+    return fail(JB_ECUDA, std::string("jb_local_create: ") + cudaGetErrorString(e));
+  }
+  *out = L;
+  return JB_OK;
+}
+
+int jb_local_destroy(jb_local* L) {
+  if (!L) return JB_OK;
+  cudaFree(L->table);
+  cudaFree(L->phase);
+  delete L;
+  return JB_OK;
+}
+
+static jb::LocalDesc local_desc(const jb_local* L) {
+  jb::LocalDesc d;
+  d.phase = L->phase;
+  d.index_bytes = L->index_bytes;
+  d.table = L->table;
+  d.dim = L->dim;
+  return d;
+}
+
+int jb_local_apply(jb_local* L, const void* x, void* y, int64_t batch, void* stream) {
+  if (!L || !x || !y) return fail(JB_EINVAL, "NULL argument");
+  if (batch < 1) return fail(JB_EINVAL, "batch must be >= 1");
+  const int C = L->dim == 2 ? 3 : 6;
+  return launch_status(jb::launch_local(L->dtype, local_desc(L), C, (int)batch, L->nvox, x, y,
+                                        as_stream(stream)),
+                       "local");
+}
+
+int jb_block_linear_apply(int dtype, int64_t nvox, int osz, int isz, const void* a,
+                          const void* x, void* y, int transpose, void* stream) {
+  if (!a || !x || !y) return fail(JB_EINVAL, "NULL argument");
+  if (dtype != F64 && dtype != F32) return fail(JB_EINVAL, "dtype must be JB_F64 or JB_F32");
+  if (nvox < 0 || osz < 1 || isz < 1 || osz > 8 || isz > 8)
+    return fail(JB_EINVAL, "block sizes must be in [1, 8]");
+  if (nvox == 0) return JB_OK;
+  return launch_status(jb::launch_block_linear(dtype, nvox, 1, osz, isz, a, x, y, transpose,
+                                               as_stream(stream)),
+                       "block_linear");
+}
+
+// ---------------------------------------------------------------------------
+// basic fixed-point scheme
+// ---------------------------------------------------------------------------
+
+int jb_solver_create(jb_green* G, jb_local* L, int nload, jb_solver** out) {
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  if (!G || !L) return fail(JB_EINVAL, "NULL argument");
+  if (nload < 1 || nload > 65535) return fail(JB_EINVAL, "nload must be in [1, 65535]");
+  if (G->dim != L->dim || G->dtype != L->dtype)
+    return fail(JB_EINVAL, "green and local operators differ in dim or dtype");
+  for (int d = 0; d < G->dim; ++d)
+    if (G->n[d] != L->n[d]) return fail(JB_EINVAL, "green and local operators differ in shape");
+  jb_solver* S = new jb_solver();
+  S->green = G;
+  S->local = L;
+  S->L = nload;
+  const int C = G->dim == 2 ? 3 : 6;
+  int r = ensure_buf(S->spec, (size_t)nload * spec_elems(G) * 2 * real_size(G->dtype));
+  if (r == JB_OK) r = ensure_buf(S->E, sizeof(double) * nload * C);
+  if (r == JB_OK) r = ensure_buf(S->res, sizeof(double) * nload);
+  if (r == JB_OK) r = ensure_buf(S->mean, sizeof(double) * nload * C);
+  if (r == JB_OK) r = ensure_buf(S->normd, sizeof(double) * nload);
+  // partials: rows_c2r grid (<= rows) and local_sum grid (<= 1024 per comp)
+  const int64_t rows = G->dim == 2 ? G->n[0] : G->n[0] * G->n[1];
+  const int64_t np = std::max<int64_t>(rows, 1024 * C);
+  if (r == JB_OK) r = ensure_buf(S->partials, sizeof(double) * nload * np);
+  if (r != JB_OK) {
+    jb_solver_destroy(S);
+    return r;
+  }
+  *out = S;
+  return JB_OK;
+}
+
+int jb_solver_destroy(jb_solver* S) {
+  if (!S) return JB_OK;
+  for (DeviceBuf* b : {&S->spec, &S->partials, &S->E, &S->res, &S->mean, &S->normd})
+    if (b->p) cudaFree(b->p);
+  delete S;
+  return JB_OK;
+}
+
+int jb_solver_set_load(jb_solver* S, const double* E) {
+  if (!S || !E) return fail(JB_EINVAL, "NULL argument");
+  const int C = S->green->dim == 2 ? 3 : 6;
+  double N = 1;
+  for (int d = 0; d < S->green->dim; ++d) N *= (double)S->green->n[d];
+  S->Eh.assign(E, E + (size_t)S->L * C);
+  S->norm.resize(S->L);
+  for (int l = 0; l < S->L; ++l) {
+    double s = 0;
+    for (int c = 0; c < C; ++c) s += E[l * C + c] * E[l * C + c];
+    if (!(s > 0)) return fail(JB_EINVAL, "macroscopic strain must be nonzero");
+    S->norm[l] = 1.0 / std::sqrt(N) / std::sqrt(s);  // square_basic.py:86
+  }
+  JB_CUDA(cudaMemcpy(S->E.p, E, sizeof(double) * S->L * C, cudaMemcpyHostToDevice));
+  JB_CUDA(cudaMemcpy(S->normd.p, S->norm.data(), sizeof(double) * S->L, cudaMemcpyHostToDevice));
+  S->load_set = true;
+  return JB_OK;
+}
+
+int jb_solver_step(jb_solver* S, void* eps, double* res_dev, void* stream) {
+  if (!S || !eps) return fail(JB_EINVAL, "NULL argument");
+  if (!S->load_set) return fail(JB_ESTATE, "jb_solver_set_load must be called first");
+  cudaStream_t st = as_stream(stream);
+  jb::LocalDesc loc = local_desc(S->local);
+  jb::UpdateDesc upd;
+  upd.eps = eps;
+  upd.E = static_cast<const double*>(S->E.p);
+  upd.partials = static_cast<double*>(S->partials.p);
+  int nb = 0;
+  JB_TRY(green_passes(S->green, eps, eps, S->L, S->spec.p, &loc, &upd, &nb, st));
+  if (res_dev) {
+    JB_TRY(launch_status(jb::launch_reduce_rows(static_cast<const double*>(S->partials.p), S->L,
+                                                nb, res_dev, 1.0,
+                                                static_cast<const double*>(S->normd.p), 1, st),
+                         "reduce"));
+  }
+  S->nb_rows = nb;
+  return JB_OK;
+}
+
+int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_iter, double tol,
+                  double* residuals, int* iters_out, double* mean_tau, void* stream) {
+  if (!S || !E || !eps) return fail(JB_EINVAL, "NULL argument");
+  if (max_iter < 0) return fail(JB_EINVAL, "max_iter must be >= 0");
+  JB_TRY(jb_solver_set_load(S, E));
+  cudaStream_t st = as_stream(stream);
+  const int C = S->green->dim == 2 ? 3 : 6;
+  const int64_t nvox = S->local->nvox;
+  if (init)
+    JB_TRY(launch_status(jb::launch_fill_macro(S->green->dtype, C, S->L, nvox,
+                                               static_cast<const double*>(S->E.p), eps, st),
+                         "fill"));
+  std::vector<double> r(S->L);
+  int it = 0;
+  for (; it < max_iter; ++it) {
+    JB_TRY(jb_solver_step(S, eps, static_cast<double*>(S->res.p), st));
+    JB_CUDA(cudaMemcpyAsync(r.data(), S->res.p, sizeof(double) * S->L, cudaMemcpyDeviceToHost,
+                            st));
+    JB_CUDA(cudaStreamSynchronize(st));
+    bool done = true;
+    for (int l = 0; l < S->L; ++l) {
+      if (residuals) residuals[(size_t)it * S->L + l] = r[l];
+      if (!(r[l] <= tol)) done = false;
+    }
+    if (done) {
+      ++it;
+      break;
+    }
+  }
+  if (iters_out) *iters_out = it;
+  if (mean_tau) {
+    int nb = 0;
+    JB_TRY(launch_status(jb::launch_local_sum(S->green->dtype, local_desc(S->local), C, S->L,
+                                              nvox, eps, static_cast<double*>(S->partials.p),
+                                              &nb, st),
+                         "local_sum"));
+    JB_TRY(launch_status(jb::launch_reduce_cols(static_cast<const double*>(S->partials.p), S->L,
+                                                C, nb, static_cast<double*>(S->mean.p),
+                                                1.0 / (double)nvox, st),
+                         "reduce"));
+    JB_CUDA(cudaMemcpyAsync(mean_tau, S->mean.p, sizeof(double) * S->L * C,
+                            cudaMemcpyDeviceToHost, st));
+  }
+  JB_CUDA(cudaStreamSynchronize(st));
+  return JB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,704 @@
+// Pass kernels of the janus_b200 Lippmann-Schwinger path (sm_100a).
+//
+// A Green-operator application y = F^-1[Gamma-hat F[x]] on an n0 x n1 (x n2)
+// grid of s-component Mandel fields is a sequence of shared-memory passes,
+// each reading and writing every spectral value once:
+//   2D: rows_r2c (axis 1) | cols mode 2 (axis 0: fwd, Gamma, inv) | rows_c2r
+//   3D: rows_r2c (axis 2) | cols fwd (axis 1) | cols mode 2 (axis 0)
+//       | cols inv (axis 1) | rows_c2r
+// The local operator (C - C0):eps is fused into rows_r2c and the solver
+// update eps = E - y/N with its FP64 residual partials into rows_c2r.
+//
+// Spectral layout in HBM: complex [L][n0][(n1)][m][s], m = n_last/2 + 1,
+// Mandel component fastest (so one spectral coefficient's s components are
+// one contiguous 48-byte (3D) / 24-byte (2D) group in FP64 complex).
+#include <mutex>
+#include <unordered_map>
+
+#include "jb_green.cuh"
+#include "jb_kernels.h"
+
+namespace jb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr size_t kSmemCap = 227 * 1024;
+constexpr size_t kSmemBudget = 96 * 1024;
+
+template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
+template <> __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <> __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+template <typename T> __device__ __forceinline__ T add_rn(T a, T b);
+template <> __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+template <> __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+template <typename T> __device__ __forceinline__ T sub_rn(T a, T b);
+template <> __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+template <> __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+// FourthRankIsotropicTensor2D/3D.c_apply (janus/operators.pyx:317-324,
+// 354-365) with the reference's operation order and no contraction into
+// FMA, so the result is bitwise that of the reference for the same inputs.
+// In place: p[0..s-1] <- (tr J' + dev I) : p.
+template <typename T>
+__device__ __forceinline__ void iso_apply(T* p, T tr, T dev, int dim) {
+  if (dim == 2) {
+    const T x0 = p[0], x1 = p[1], x2 = p[2];
+    const T aux = mul_rn(tr, add_rn(x0, x1));
+    p[0] = add_rn(aux, mul_rn(dev, x0));
+    p[1] = add_rn(aux, mul_rn(dev, x1));
+    p[2] = mul_rn(dev, x2);
+  } else {
+    const T x0 = p[0], x1 = p[1], x2 = p[2];
+    const T aux = mul_rn(tr, add_rn(add_rn(x0, x1), x2));
+    p[0] = add_rn(aux, mul_rn(dev, x0));
+    p[1] = add_rn(aux, mul_rn(dev, x1));
+    p[2] = add_rn(aux, mul_rn(dev, x2));
+    p[3] = mul_rn(dev, p[3]);
+    p[4] = mul_rn(dev, p[4]);
+    p[5] = mul_rn(dev, p[5]);
+  }
+}
+
+__device__ __forceinline__ int load_phase(const void* phase, int ib, int64_t v) {
+  return ib == 1 ? static_cast<int>(static_cast<const uint8_t*>(phase)[v])
+                 : static_cast<const int32_t*>(phase)[v];
+}
+
+// deterministic block sum (fixed shuffle tree + fixed warp order)
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) s += red[w];
+  }
+  return s;
+}
+
+template <typename T> struct RowsArgs {
+  const T* x;
+  cx<T>* out;
+  const cx<T>* cin;
+  T* y;
+  const cx<T>* tw;
+  AxisPlan plan;
+  RealGeom g;
+  int C, R, W, m;
+  int64_t cstride_l;
+  const void* phase;
+  int index_bytes;
+  const T* table;
+  int dim;
+  const double* E;
+  double* partials;
+  T scale;
+};
+
+__device__ __forceinline__ int64_t geom_off(const RealGeom& g, int64_t row, int e, int c) {
+  return (row / g.n1r) * g.s0 + (row % g.n1r) * g.s1 + e * g.es + c * g.cs;
+}
+
+template <typename T, bool LOCAL>
+__global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
+  using C = cx<T>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int n = a.plan.n, W = a.W, R = a.R, Cc = a.C, m = a.m;
+  C* tw = reinterpret_cast<C*>(smem);
+  C* A = tw + n;
+  C* B = A + (size_t)(n + 2) * W;
+  T* Ar = reinterpret_cast<T*>(A);
+  const int ldr = 2 * W;
+  const int l = blockIdx.y;
+  const int64_t row0 = (int64_t)blockIdx.x * R;
+  const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
+  const int RC = R * Cc;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  const T* xl = a.x + l * a.g.ls;
+  const int total = RC * n;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int c = idx % Cc;
+    const int t = idx / Cc;
+    const int e = t % n;
+    const int rr = t / n;
+    T v = T(0);
+    if (rr < rows_here) v = xl[geom_off(a.g, row0 + rr, e, c)];
+    Ar[e * ldr + rr * Cc + c] = v;
+  }
+  if (ldr > RC)
+    for (int e = threadIdx.x; e < n; e += blockDim.x)
+      for (int j = RC; j < ldr; ++j) Ar[e * ldr + j] = T(0);
+  __syncthreads();
+  if (LOCAL) {
+    for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
+      const int e = idx % n;
+      const int rr = idx / n;
+      if (rr < rows_here) {
+        const int ph = load_phase(a.phase, a.index_bytes, (row0 + rr) * n + e);
+        iso_apply<T>(Ar + e * ldr + rr * Cc, a.table[2 * ph], a.table[2 * ph + 1], a.dim);
+      }
+    }
+    __syncthreads();
+  }
+  C* Z = fft_tile<-1>(A, B, tw, a.plan, W);
+  C* S = (Z == A) ? B : A;
+  for (int idx = threadIdx.x; idx < m * W; idx += blockDim.x) {
+    const int col = idx % W;
+    const int k = idx / W;
+    const C P = Z[k * W + col];
+    const C Q = cconj(Z[(k == 0 ? 0 : n - k) * W + col]);
+    const int ra = 2 * col, rb = 2 * col + 1;
+    const int rra = ra / Cc, ca = ra - rra * Cc;
+    const int rrb = rb / Cc, cb = rb - rrb * Cc;
+    if (ra < RC && rra < rows_here)
+      S[((int64_t)rra * m + k) * Cc + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
+    if (rb < RC && rrb < rows_here)
+      S[((int64_t)rrb * m + k) * Cc + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
+  }
+  __syncthreads();
+  C* dst = a.out + l * a.cstride_l + row0 * m * Cc;
+  const int cnt = rows_here * m * Cc;
+  for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) dst[idx] = S[idx];
+}
+
+template <typename T, bool UPDATE>
+__global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
+  using C = cx<T>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double red[kThreads / 32];
+  const int n = a.plan.n, W = a.W, R = a.R, Cc = a.C, m = a.m;
+  C* tw = reinterpret_cast<C*>(smem);
+  C* A = tw + n;
+  C* B = A + (size_t)(n + 2) * W;
+  const int ldr = 2 * W;
+  const int l = blockIdx.y;
+  const int64_t row0 = (int64_t)blockIdx.x * R;
+  const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
+  const int RC = R * Cc;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  const C* src = a.cin + l * a.cstride_l + row0 * m * Cc;
+  const int cnt = rows_here * m * Cc;
+  for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) B[idx] = src[idx];
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
+    const int col = idx % W;
+    const int k = idx / W;
+    const int ra = 2 * col, rb = 2 * col + 1;
+    const int rra = ra / Cc, ca = ra - rra * Cc;
+    const int rrb = rb / Cc, cb = rb - rrb * Cc;
+    const bool mirror = 2 * k > n;
+    const int kk = mirror ? n - k : k;
+    C Av = mkc(T(0), T(0)), Bv = mkc(T(0), T(0));
+    if (ra < RC && rra < rows_here) Av = B[((int64_t)rra * m + kk) * Cc + ca];
+    if (rb < RC && rrb < rows_here) Bv = B[((int64_t)rrb * m + kk) * Cc + cb];
+    if (kk == 0 || 2 * kk == n) {
+      Av.y = T(0);
+      Bv.y = T(0);
+    }
+    A[k * W + col] = mirror ? mkc(Av.x + Bv.y, Bv.x - Av.y) : mkc(Av.x - Bv.y, Av.y + Bv.x);
+  }
+  __syncthreads();
+  C* Z = fft_tile<+1>(A, B, tw, a.plan, W);
+  const T* Zr = reinterpret_cast<const T*>(Z);
+  double acc = 0.0;
+  T* yl = UPDATE ? nullptr : a.y + l * a.g.ls;
+  T* el = UPDATE ? reinterpret_cast<T*>(a.y) + l * a.g.ls : nullptr;
+  const int total = RC * n;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int c = idx % Cc;
+    const int t = idx / Cc;
+    const int e = t % n;
+    const int rr = t / n;
+    if (rr < rows_here) {
+      const T v = Zr[e * ldr + rr * Cc + c];
+      const int64_t off = geom_off(a.g, row0 + rr, e, c);
+      if (UPDATE) {
+        const T old = el[off];
+        const T nv = sub_rn(static_cast<T>(a.E[l * Cc + c]), mul_rn(a.scale, v));
+        el[off] = nv;
+        const double d = static_cast<double>(nv) - static_cast<double>(old);
+        acc += d * d;
+      } else {
+        yl[off] = mul_rn(a.scale, v);
+      }
+    }
+  }
+  if (UPDATE) {
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) a.partials[(int64_t)l * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+template <typename T> struct ColsArgs {
+  const cx<T>* in;
+  cx<T>* out;
+  const cx<T>* tw;
+  AxisPlan plan;
+  int64_t inner;
+  int W, C;
+  int64_t m_last;
+  GreenTables<T> gt;
+};
+
+template <typename T, int MODE, int DIM>
+__global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
+  using C = cx<T>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int n = a.plan.n, W = a.W;
+  C* tw = reinterpret_cast<C*>(smem);
+  C* A = tw + n;
+  C* B = A + (size_t)n * W;
+  const int64_t c0 = (int64_t)blockIdx.x * W;
+  const int Wc = (int)min((int64_t)W, a.inner - c0);
+  const int64_t o = blockIdx.y;
+  const C* src = a.in + o * n * a.inner + c0;
+  C* dst = a.out + o * n * a.inner + c0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
+    const int e = idx / W;
+    const int col = idx - e * W;
+    A[idx] = col < Wc ? src[(int64_t)e * a.inner + col] : mkc(T(0), T(0));
+  }
+  __syncthreads();
+  C* Z;
+  if (MODE == 1)
+    Z = fft_tile<+1>(A, B, tw, a.plan, W);
+  else
+    Z = fft_tile<-1>(A, B, tw, a.plan, W);
+  if (MODE == 2) {
+    const int Cc = a.C;
+    const int Wf = W / Cc;
+    for (int idx = threadIdx.x; idx < n * Wf; idx += blockDim.x) {
+      const int e = idx / Wf;
+      const int fl = idx - e * Wf;
+      const int col0 = fl * Cc;
+      if (col0 < Wc) {
+        const int64_t f = (c0 + col0) / Cc;
+        int b[3];
+        b[0] = e;
+        if (DIM == 3) {
+          b[1] = (int)(f / a.m_last);
+          b[2] = (int)(f % a.m_last);
+        } else {
+          b[1] = (int)f;
+          b[2] = 0;
+        }
+        green_contract<DIM, T>(a.gt, b, Z + e * W + col0);
+      }
+    }
+    __syncthreads();
+    C* other = (Z == A) ? B : A;
+    Z = fft_tile<+1>(Z, other, tw, a.plan, W);
+  }
+  for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
+    const int e = idx / W;
+    const int col = idx - e * W;
+    if (col < Wc) dst[(int64_t)e * a.inner + col] = Z[idx];
+  }
+}
+
+template <typename T>
+__global__ void local_kernel(LocalDesc loc, const T* table, int C, int L, int64_t nvox,
+                             const T* x, T* y) {
+  const int64_t total = (int64_t)L * nvox;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i % nvox;
+    const int ph = load_phase(loc.phase, loc.index_bytes, v);
+    T p[6];
+    for (int c = 0; c < C; ++c) p[c] = x[i * C + c];
+    iso_apply<T>(p, table[2 * ph], table[2 * ph + 1], loc.dim);
+    for (int c = 0; c < C; ++c) y[i * C + c] = p[c];
+  }
+}
+
+template <typename T>
+__global__ void local_sum_kernel(LocalDesc loc, const T* table, int C, int64_t nvox,
+                                 const T* eps, double* partials) {
+  __shared__ double red[kThreads / 32];
+  const int l = blockIdx.y;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const T* el = eps + (int64_t)l * nvox * C;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int ph = load_phase(loc.phase, loc.index_bytes, v);
+    T p[6];
+    for (int c = 0; c < C; ++c) p[c] = el[v * C + c];
+    iso_apply<T>(p, table[2 * ph], table[2 * ph + 1], loc.dim);
+    for (int c = 0; c < C; ++c) acc[c] += static_cast<double>(p[c]);
+  }
+  for (int c = 0; c < C; ++c) {
+    const double s = block_sum(acc[c], red);
+    if (threadIdx.x == 0) partials[((int64_t)l * C + c) * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+template <typename T>
+__global__ void block_linear_kernel(int64_t nvox, int L, int osz, int isz, const T* a,
+                                    const T* x, T* y, int transpose) {
+  const int64_t total = (int64_t)L * nvox;
+  const int ni = transpose ? osz : isz;  // length of x per voxel
+  const int no = transpose ? isz : osz;  // length of y per voxel
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i % nvox;
+    const T* av = a + v * osz * isz;
+    const T* xv = x + i * ni;
+    T xl[8];
+    for (int j = 0; j < ni; ++j) xl[j] = xv[j];
+    T* yv = y + i * no;
+    for (int r = 0; r < no; ++r) {
+      T s = T(0);
+      for (int j = 0; j < ni; ++j)
+        s = add_rn(s, mul_rn(transpose ? av[j * isz + r] : av[r * isz + j], xl[j]));
+      yv[r] = s;
+    }
+  }
+}
+
+template <typename T, int DIM>
+__global__ void green_by_freq_kernel(GreenTables<T> gt, int64_t count, const int* b,
+                                     const cx<T>* tau, cx<T>* eta) {
+  constexpr int S = DIM == 2 ? 3 : 6;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    cx<T> t[S];
+    for (int c = 0; c < S; ++c) t[c] = tau[i * S + c];
+    int bb[3] = {b[i * DIM], b[i * DIM + 1], DIM == 3 ? b[i * DIM + 2] : 0};
+    green_contract<DIM, T>(gt, bb, t);
+    for (int c = 0; c < S; ++c) eta[i * S + c] = t[c];
+  }
+}
+
+template <typename T>
+__global__ void fill_macro_kernel(int C, int L, int64_t nvox, const double* E, T* eps) {
+  const int64_t total = (int64_t)L * nvox * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const int l = (int)(i / (nvox * C));
+    eps[i] = static_cast<T>(E[l * C + c]);
+  }
+}
+
+__global__ void reduce_rows_kernel(const double* partials, int nb, double* out, double factor,
+                                   const double* factors, int take_sqrt) {
+  __shared__ double red[kThreads / 32];
+  const int l = blockIdx.x;
+  double acc = 0.0;
+  // fixed assignment of partials to threads, fixed tree: deterministic
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += partials[(int64_t)l * nb + i];
+  const double s = block_sum(acc, red);
+  if (threadIdx.x == 0) {
+    const double f = factors ? factor * factors[l] : factor;
+    out[l] = take_sqrt ? sqrt(s) * f : s * f;
+  }
+}
+
+std::mutex g_attr_mu;
+std::unordered_map<const void*, size_t> g_attr;
+
+cudaError_t ensure_smem(const void* fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  auto it = g_attr.find(fn);
+  if (it != g_attr.end() && it->second >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSmemCap);
+  if (e == cudaSuccess) g_attr[fn] = kSmemCap;
+  return e;
+}
+
+int grid_for(int64_t total) {
+  int64_t g = (total + kThreads - 1) / kThreads;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// rows per CTA and tile width for the contiguous-axis kernels
+bool rows_shape(int dtype, int n, int C, int* R, int* W, size_t* smem) {
+  const size_t cs = dtype == F64 ? 16 : 8;
+  int r = (24 + C - 1) / C;
+  for (;;) {
+    const int w = (r * C + 1) / 2;
+    const size_t bytes = n * cs + 2 * (size_t)(n + 2) * w * cs;
+    if (bytes <= kSmemBudget || r == 1) {
+      if (bytes > kSmemCap - 4096) return false;
+      *R = r;
+      *W = w;
+      *smem = bytes;
+      return true;
+    }
+    --r;
+  }
+}
+
+bool cols_shape(int dtype, int n, int unit, int* W, size_t* smem) {
+  const size_t cs = dtype == F64 ? 16 : 8;
+  int w = unit * ((16 + unit / 2) / unit);
+  if (w < unit) w = unit;
+  for (;;) {
+    const size_t bytes = n * cs + 2 * (size_t)n * w * cs;
+    if (bytes <= kSmemBudget || w == unit) {
+      if (bytes > kSmemCap - 4096) return false;
+      *W = w;
+      *smem = bytes;
+      return true;
+    }
+    w -= unit;
+  }
+}
+
+template <typename T>
+cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const RealGeom& g,
+                       void* out, const LocalDesc* local, cudaStream_t st) {
+  RowsArgs<T> a{};
+  int R, W;
+  size_t smem;
+  const int n = ax.plan.n;
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, &R, &W, &smem)) return cudaErrorInvalidValue;
+  a.x = static_cast<const T*>(x);
+  a.out = static_cast<cx<T>*>(out);
+  a.tw = static_cast<const cx<T>*>(ax.tw);
+  a.plan = ax.plan;
+  a.g = g;
+  a.C = C;
+  a.R = R;
+  a.W = W;
+  a.m = n / 2 + 1;
+  a.cstride_l = g.rows * a.m * C;
+  dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
+  if (local) {
+    a.phase = local->phase;
+    a.index_bytes = local->index_bytes;
+    a.table = static_cast<const T*>(local->table);
+    a.dim = local->dim;
+    const void* fn = reinterpret_cast<const void*>(&rows_r2c_kernel<T, true>);
+    cudaError_t e = ensure_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    rows_r2c_kernel<T, true><<<grid, kThreads, smem, st>>>(a);
+  } else {
+    const void* fn = reinterpret_cast<const void*>(&rows_r2c_kernel<T, false>);
+    cudaError_t e = ensure_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    rows_r2c_kernel<T, false><<<grid, kThreads, smem, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y,
+                       const RealGeom& g, double scale, const UpdateDesc* upd, int* nb_out,
+                       cudaStream_t st) {
+  RowsArgs<T> a{};
+  int R, W;
+  size_t smem;
+  const int n = ax.plan.n;
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, &R, &W, &smem)) return cudaErrorInvalidValue;
+  a.cin = static_cast<const cx<T>*>(in);
+  a.y = static_cast<T*>(upd ? upd->eps : y);
+  a.tw = static_cast<const cx<T>*>(ax.tw);
+  a.plan = ax.plan;
+  a.g = g;
+  a.C = C;
+  a.R = R;
+  a.W = W;
+  a.m = n / 2 + 1;
+  a.cstride_l = g.rows * a.m * C;
+  a.scale = static_cast<T>(scale);
+  dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
+  if (nb_out) *nb_out = (int)grid.x;
+  if (upd) {
+    a.E = upd->E;
+    a.partials = upd->partials;
+    const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, true>);
+    cudaError_t e = ensure_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    rows_c2r_kernel<T, true><<<grid, kThreads, smem, st>>>(a);
+  } else {
+    const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, false>);
+    cudaError_t e = ensure_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    rows_c2r_kernel<T, false><<<grid, kThreads, smem, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T> GreenTables<T> to_tables(const GreenDeviceTables* gt) {
+  GreenTables<T> t{};
+  if (!gt) return t;
+  for (int d = 0; d < 3; ++d) {
+    t.kt[d] = static_cast<const T*>(gt->kt[d]);
+    t.kn[d] = static_cast<const T*>(gt->kn[d]);
+    t.kp[d] = static_cast<const T*>(gt->kp[d]);
+    t.wn[d] = static_cast<const T*>(gt->wn[d]);
+    t.wp[d] = static_cast<const T*>(gt->wp[d]);
+  }
+  t.inv2g = static_cast<T>(gt->inv2g);
+  t.c1 = static_cast<T>(gt->c1);
+  t.variant = gt->variant;
+  return t;
+}
+
+template <typename T, int MODE, int DIM>
+cudaError_t cols_launch(const ColsArgs<T>& a, dim3 grid, size_t smem, cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(&cols_kernel<T, MODE, DIM>);
+  cudaError_t e = ensure_smem(fn, smem);
+  if (e != cudaSuccess) return e;
+  cols_kernel<T, MODE, DIM><<<grid, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, const void* in,
+                   void* out, int C, int dim, const GreenDeviceTables* gt, int64_t m_last,
+                   cudaStream_t st) {
+  ColsArgs<T> a{};
+  int W;
+  size_t smem;
+  const int n = ax.plan.n;
+  if (outer < 1 || outer > 65535 || inner < 1) return cudaErrorInvalidValue;
+  if (mode == 2 && (inner % C) != 0) return cudaErrorInvalidValue;
+  if (!cols_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &W, &smem))
+    return cudaErrorInvalidValue;
+  a.in = static_cast<const cx<T>*>(in);
+  a.out = static_cast<cx<T>*>(out);
+  a.tw = static_cast<const cx<T>*>(ax.tw);
+  a.plan = ax.plan;
+  a.inner = inner;
+  a.W = W;
+  a.C = C;
+  a.m_last = m_last;
+  a.gt = to_tables<T>(gt);
+  dim3 grid((unsigned)((inner + W - 1) / W), (unsigned)outer);
+  if (mode == 0) return cols_launch<T, 0, 2>(a, grid, smem, st);
+  if (mode == 1) return cols_launch<T, 1, 2>(a, grid, smem, st);
+  if (dim == 2) return cols_launch<T, 2, 2>(a, grid, smem, st);
+  return cols_launch<T, 2, 3>(a, grid, smem, st);
+}
+
+}  // namespace
+
+int max_axis_length(int dtype) { return dtype == F64 ? 4096 : 8192; }
+
+cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const void* x,
+                            const RealGeom& g, void* out, const LocalDesc* local,
+                            cudaStream_t st) {
+  return dtype == F64 ? rows_r2c_t<double>(ax, C, L, x, g, out, local, st)
+                      : rows_r2c_t<float>(ax, C, L, x, g, out, local, st);
+}
+
+cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const void* in,
+                            void* y, const RealGeom& g, double scale, const UpdateDesc* upd,
+                            int* nb_out, cudaStream_t st) {
+  return dtype == F64 ? rows_c2r_t<double>(ax, C, L, in, y, g, scale, upd, nb_out, st)
+                      : rows_c2r_t<float>(ax, C, L, in, y, g, scale, upd, nb_out, st);
+}
+
+cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer, int64_t inner,
+                        const void* in, void* out, int C, int dim,
+                        const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
+                        cudaStream_t st) {
+  (void)n1;
+  return dtype == F64 ? cols_t<double>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st)
+                      : cols_t<float>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st);
+}
+
+cudaError_t launch_local(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
+                         const void* x, void* y, cudaStream_t st) {
+  const int grid = grid_for((int64_t)L * nvox);
+  if (dtype == F64)
+    local_kernel<double><<<grid, kThreads, 0, st>>>(loc, static_cast<const double*>(loc.table),
+                                                    C, L, nvox, static_cast<const double*>(x),
+                                                    static_cast<double*>(y));
+  else
+    local_kernel<float><<<grid, kThreads, 0, st>>>(loc, static_cast<const float*>(loc.table), C,
+                                                   L, nvox, static_cast<const float*>(x),
+                                                   static_cast<float*>(y));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_local_sum(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
+                             const void* eps, double* partials, int* nb_out, cudaStream_t st) {
+  int g = grid_for(nvox);
+  if (g > 1024) g = 1024;
+  *nb_out = g;
+  dim3 grid((unsigned)g, (unsigned)L);
+  if (dtype == F64)
+    local_sum_kernel<double><<<grid, kThreads, 0, st>>>(
+        loc, static_cast<const double*>(loc.table), C, nvox, static_cast<const double*>(eps),
+        partials);
+  else
+    local_sum_kernel<float><<<grid, kThreads, 0, st>>>(
+        loc, static_cast<const float*>(loc.table), C, nvox, static_cast<const float*>(eps),
+        partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_linear(int dtype, int64_t nvox, int L, int osz, int isz, const void* a,
+                                const void* x, void* y, int transpose, cudaStream_t st) {
+  if (osz > 8 || isz > 8) return cudaErrorInvalidValue;
+  const int grid = grid_for((int64_t)L * nvox);
+  if (dtype == F64)
+    block_linear_kernel<double><<<grid, kThreads, 0, st>>>(
+        nvox, L, osz, isz, static_cast<const double*>(a), static_cast<const double*>(x),
+        static_cast<double*>(y), transpose);
+  else
+    block_linear_kernel<float><<<grid, kThreads, 0, st>>>(
+        nvox, L, osz, isz, static_cast<const float*>(a), static_cast<const float*>(x),
+        static_cast<float*>(y), transpose);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_green_by_freq(int dtype, int dim, const GreenDeviceTables& gt, int64_t count,
+                                 const int* b, const void* tau, void* eta, cudaStream_t st) {
+  const int grid = grid_for(count);
+  if (dtype == F64) {
+    auto t = to_tables<double>(&gt);
+    if (dim == 2)
+      green_by_freq_kernel<double, 2><<<grid, kThreads, 0, st>>>(
+          t, count, b, static_cast<const double2*>(tau), static_cast<double2*>(eta));
+    else
+      green_by_freq_kernel<double, 3><<<grid, kThreads, 0, st>>>(
+          t, count, b, static_cast<const double2*>(tau), static_cast<double2*>(eta));
+  } else {
+    auto t = to_tables<float>(&gt);
+    if (dim == 2)
+      green_by_freq_kernel<float, 2><<<grid, kThreads, 0, st>>>(
+          t, count, b, static_cast<const float2*>(tau), static_cast<float2*>(eta));
+    else
+      green_by_freq_kernel<float, 3><<<grid, kThreads, 0, st>>>(
+          t, count, b, static_cast<const float2*>(tau), static_cast<float2*>(eta));
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_macro(int dtype, int C, int L, int64_t nvox, const double* E, void* eps,
+                              cudaStream_t st) {
+  const int grid = grid_for((int64_t)L * nvox * C);
+  if (dtype == F64)
+    fill_macro_kernel<double><<<grid, kThreads, 0, st>>>(C, L, nvox, E, static_cast<double*>(eps));
+  else
+    fill_macro_kernel<float><<<grid, kThreads, 0, st>>>(C, L, nvox, E, static_cast<float*>(eps));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_rows(const double* partials, int L, int nb, double* out, double factor,
+                               const double* factors, int take_sqrt, cudaStream_t st) {
+  reduce_rows_kernel<<<L, kThreads, 0, st>>>(partials, nb, out, factor, factors, take_sqrt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_cols(const double* partials, int L, int C, int nb, double* out,
+                               double factor, cudaStream_t st) {
+  reduce_rows_kernel<<<L * C, kThreads, 0, st>>>(partials, nb, out, factor, nullptr, 0);
+  return cudaGetLastError();
+}
+
+}  // namespace jb

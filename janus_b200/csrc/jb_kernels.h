@@ -1,0 +1,102 @@
+// Host-side launch interface of the janus_b200 pass kernels (internal; the
+// public interface is the C ABI in include/janus_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "jb_device.cuh"
+
+namespace jb {
+
+enum Dtype { F64 = 0, F32 = 1 };
+enum Variant { TRUNCATED = 0, FILTERED = 1 };
+
+// per-axis FFT data: plan + device twiddle table (T complex, n entries)
+struct AxisData {
+  AxisPlan plan;
+  void* tw = nullptr;  // device, cx<T>[n]
+};
+
+// discrete Green operator tables on the device (type T)
+struct GreenDeviceTables {
+  void* kt[3] = {nullptr, nullptr, nullptr};
+  void* kn[3] = {nullptr, nullptr, nullptr};
+  void* kp[3] = {nullptr, nullptr, nullptr};
+  void* wn[3] = {nullptr, nullptr, nullptr};
+  void* wp[3] = {nullptr, nullptr, nullptr};
+  double inv2g = 0, c1 = 0;
+  int variant = 0;
+};
+
+// Real-side geometry of a batch of fields [L][rows][n][C] with arbitrary
+// element strides: element (l, row, e, c) lives at
+//   l*ls + (row / n1r)*s0 + (row % n1r)*s1 + e*es + c*cs.
+struct RealGeom {
+  int64_t rows;  // rows per load case (n0 or n0*n1)
+  int64_t n1r;   // 1 (2D) or n1 (3D)
+  int64_t ls, s0, s1, es, cs;
+};
+
+// Local operator (C - C0):eps on a phase map; table holds (tr, dev) pairs
+// in the field's precision.
+struct LocalDesc {
+  const void* phase = nullptr;  // uint8 or int32 per voxel, row-major grid
+  int index_bytes = 1;          // 1 or 4
+  const void* table = nullptr;  // device, T[2 * nphase]
+  int dim = 2;
+};
+
+// Solver update of the last pass: eps = E - scale * y, residual partials.
+struct UpdateDesc {
+  void* eps = nullptr;          // field updated in place (layout of RealGeom)
+  const double* E = nullptr;    // device [L][C] macroscopic strains (FP64)
+  double* partials = nullptr;   // device [L][gridDim.x]
+};
+
+int max_axis_length(int dtype);
+
+// r2c along the contiguous axis: real x (geom) -> complex out [L][rows][m][C].
+cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const void* x,
+                            const RealGeom& g, void* out, const LocalDesc* local,
+                            cudaStream_t st);
+// c2r along the contiguous axis: complex in [L][rows][m][C] -> real y (geom),
+// y = scale * c2r(in), or the solver update when upd != nullptr.
+cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const void* in,
+                            void* y, const RealGeom& g, double scale,
+                            const UpdateDesc* upd, int* nblocks_out, cudaStream_t st);
+// complex transform along a strided axis of [outer][n][inner] (complex units).
+// mode 0: forward, 1: inverse, 2: forward -> Green contraction -> inverse
+// (axis 0 only; dim/m_last/grid describe the spectrum for the contraction).
+cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer,
+                        int64_t inner, const void* in, void* out, int C, int dim,
+                        const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
+                        cudaStream_t st);
+// y[l][v] = (C - C0)(v) : x[l][v] on a phase map (contiguous fields)
+cudaError_t launch_local(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
+                         const void* x, void* y, cudaStream_t st);
+// per-voxel matrices: y[l][v] = a[v] x[l][v] (or a[v]^T x[l][v])
+cudaError_t launch_block_linear(int dtype, int64_t nvox, int L, int osz, int isz,
+                                const void* a, const void* x, void* y, int transpose,
+                                cudaStream_t st);
+// Green contraction at an explicit list of indices b (int32 [count][dim]),
+// tau/eta complex [count][C] (may alias)
+cudaError_t launch_green_by_freq(int dtype, int dim, const GreenDeviceTables& gt,
+                                 int64_t count, const int* b, const void* tau, void* eta,
+                                 cudaStream_t st);
+// eps[l][v][c] = E[l][c]
+cudaError_t launch_fill_macro(int dtype, int C, int L, int64_t nvox, const double* E,
+                              void* eps, cudaStream_t st);
+// out[l] = f(sum_b partials[l][b]) * factor * (factors ? factors[l] : 1),
+// f = sqrt or identity; fixed summation order (deterministic)
+cudaError_t launch_reduce_rows(const double* partials, int L, int nb, double* out,
+                               double factor, const double* factors, int take_sqrt,
+                               cudaStream_t st);
+// sum over voxels of (C - C0):eps, per load case and component (FP64 partials)
+cudaError_t launch_local_sum(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
+                             const void* eps, double* partials, int* nblocks_out,
+                             cudaStream_t st);
+cudaError_t launch_reduce_cols(const double* partials, int L, int C, int nb, double* out,
+                               double factor, cudaStream_t st);
+
+}  // namespace jb

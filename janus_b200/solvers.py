@@ -1,0 +1,135 @@
+"""The basic fixed-point scheme for the Lippmann-Schwinger equation.
+
+The reference library has no solver function: its tutorial loop
+(sphinx/tutorials/square_basic/square_basic.py:83-97) composes the local
+operator and the Green operator,
+
+    eps_0 = E,   eps_{k+1} = E - Gamma0[(C - C0):eps_k],
+    res_k = ||eps_{k+1} - eps_k|| / (sqrt(N) ||E||),
+
+and post-processes <tau> = mean((C - C0):eps) into the effective stiffness
+(square_basic.py:95-97).  ``BasicScheme`` runs exactly that loop on the GPU
+for several macroscopic load cases at once, with each iteration as five
+(3D) or three (2D) fused passes: the local operator inside the first FFT
+pass and the update plus FP64 residual reduction inside the last.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _arrays as A
+from . import _lib
+from .operators import LocalPhaseOperator, _BlockDiagonalOperator
+
+
+@dataclass
+class SolveResult:
+    eps: torch.Tensor          # (nload,) + grid + (s,) on the device
+    residuals: np.ndarray      # (iterations, nload)
+    iterations: int
+    mean_tau: np.ndarray       # (nload, s): grid mean of (C - C0):eps
+
+    def mean_stress(self, mat0, avg_eps):
+        """<sigma> = C0:E + <tau> (square_basic.py:95-96, Mandel form)."""
+        return _c0_apply(mat0, np.atleast_2d(avg_eps)) + self.mean_tau
+
+
+def _c0_apply(mat0, E):
+    dim = mat0.dim
+    sph, dev = dim * mat0.k, 2 * mat0.g
+    tr = (sph - dev) / dim
+    out = dev * E
+    out[:, :dim] += tr * E[:, :dim].sum(axis=1, keepdims=True)
+    return out
+
+
+class BasicScheme:
+    """Basic scheme on `nload` load cases with a Green operator from
+    janus_b200.green and a phase-map local operator."""
+
+    def __init__(self, green_op, local_op, nload=1):
+        if isinstance(local_op, _BlockDiagonalOperator):
+            local = local_op.local
+            if local is None:
+                raise ValueError("the solver needs isotropic local operators (phase map)")
+        elif isinstance(local_op, LocalPhaseOperator):
+            local = local_op
+        else:
+            raise TypeError("local_op must be a BlockDiagonalOperator or LocalPhaseOperator")
+        if tuple(local.shape) != tuple(green_op.ishape[:-1]):
+            raise ValueError("local and green operators must share the grid")
+        self.green_op = green_op
+        self.local = local
+        self.nload = int(nload)
+        self.dtype = green_op.dtype
+        if local.dtype != self.dtype:
+            raise ValueError("local and green operators must share the dtype")
+        self._handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().jb_solver_create(green_op.handle, local.handle, self.nload,
+                                               ctypes.byref(self._handle)))
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().jb_solver_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    @property
+    def field_shape(self):
+        return (self.nload,) + tuple(self.green_op.ishape)
+
+    def _macro(self, avg_eps):
+        E = np.ascontiguousarray(np.asarray(avg_eps, dtype=np.float64).reshape(
+            self.nload, self.green_op.ishape[-1]))
+        return E
+
+    def new_field(self):
+        return torch.empty(self.field_shape, dtype=self.dtype, device=A.device())
+
+    def run(self, avg_eps, num_iter, tol=0.0, eps=None, init=None):
+        """Iterate until every load case has res <= tol, at most num_iter
+        times.  eps (device tensor of field_shape) is updated in place; if
+        omitted a new field set to E is used."""
+        E = self._macro(avg_eps)
+        if eps is None:
+            eps = self.new_field()
+            init = True if init is None else init
+        elif tuple(eps.shape) != self.field_shape or eps.dtype != self.dtype or \
+                not eps.is_contiguous() or eps.device.type != "cuda":
+            raise ValueError("eps must be a contiguous CUDA tensor of shape {0}".format(
+                self.field_shape))
+        res = np.zeros((max(int(num_iter), 1), self.nload))
+        it = ctypes.c_int(0)
+        mean = np.zeros((self.nload, self.green_op.ishape[-1]))
+        P = ctypes.POINTER(ctypes.c_double)
+        _lib.check(_lib.lib().jb_solver_run(
+            self._handle, E.ctypes.data_as(P), ctypes.c_void_p(eps.data_ptr()), int(bool(init)),
+            int(num_iter), float(tol), res.ctypes.data_as(P), ctypes.byref(it),
+            mean.ctypes.data_as(P), ctypes.c_void_p(A.stream_handle())))
+        n = it.value
+        return SolveResult(eps=eps, residuals=res[:n].copy(), iterations=n, mean_tau=mean)
+
+    def set_load(self, avg_eps):
+        E = self._macro(avg_eps)
+        _lib.check(_lib.lib().jb_solver_set_load(
+            self._handle, E.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def step(self, eps, res_dev=None):
+        """One asynchronous iteration on the current stream (after set_load)."""
+        _lib.check(_lib.lib().jb_solver_step(
+            self._handle, ctypes.c_void_p(eps.data_ptr()),
+            ctypes.c_void_p(res_dev.data_ptr() if res_dev is not None else 0),
+            ctypes.c_void_p(A.stream_handle())))
+
+
+def basic_scheme(green_op, local_op, avg_eps, num_iter, tol=0.0, eps=None):
+    """Run the basic scheme for one or several load cases (rows of avg_eps)."""
+    E = np.atleast_2d(np.asarray(avg_eps, dtype=np.float64))
+    return BasicScheme(green_op, local_op, E.shape[0]).run(E, num_iter, tol, eps)
