@@ -1,0 +1,487 @@
+#!/usr/bin/env python
+"""Benchmark of the Lippmann-Schwinger basic scheme on B200.
+
+Workload (one GPU): 3D two-phase random spheres on a 128^3 grid (radius 8,
+non-overlapping, volume fraction 0.3, seeded random sequential addition),
+matrix mu=1 nu=0.3, spheres mu=100 nu=0.2, reference medium mu0=50.5
+nu0=0.3, filtered Green operator, FP64, the 6 unit macroscopic load cases
+iterated together.  One step = one basic-scheme iteration of all 6 load
+cases (6 * 128^3 voxel-iterations); the metric is voxel-iterations/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (launched with torchrun): every rank solves its own replica (no
+collective on the data path, weak scaling); the time is the max over ranks.
+``--impl reference`` times the reference's own CPU path (its Cython modules
+built in oracle/_ref, else the oracle's numpy restatement) on the same
+workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "3D LS solve voxel-iter/s & time-to-1e-8 residual, mixed vs FP64; % HBM peak"
+UNIT = "voxel-iter/s"
+FALLBACK_HBM_GBS = 6650.0
+
+MATRIX = (1.0, 0.3)
+INCLUSION = (100.0, 0.2)
+REF_MEDIUM = (50.5, 0.3)
+
+# algorithmic bytes per voxel and load case of each pass (FP64, s = 6):
+# r2c reads eps (48 B) + phase id (1 B) and writes the spectrum (48 B);
+# column passes read and write the spectrum; c2r reads the spectrum and the
+# old eps and writes the new eps.  Sum: 11*s*p + m = 529 B per voxel-iteration.
+def pass_bytes(s, p, m=1):
+    return {"rows_r2c_local": (2 * s * p + m), "cols_fwd_axis1": 2 * s * p,
+            "cols_green_axis0": 2 * s * p, "cols_inv_axis1": 2 * s * p,
+            "rows_c2r_update": 3 * s * p, "reduce_residual": 0}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(n, seed, variant, dtype):
+    import numpy as np
+
+    import janus_b200.material.elastic.linear.isotropic as material
+    from janus_b200 import microstructures as micro
+    from janus_b200 import operators as ops
+    from janus_b200.green import filtered, truncated
+
+    phase, centres = micro.random_spheres(n, radius=8 * n / 128, volume_fraction=0.3,
+                                          seed=seed)
+    mat0 = material.create(*REF_MEDIUM, 3)
+    tens = []
+    for g, nu in (MATRIX, INCLUSION):
+        m = material.create(g, nu, 3)
+        tens.append(ops.isotropic_4(3 * (m.k - mat0.k), 2 * (m.g - mat0.g), 3))
+    factory = filtered if variant == "filtered" else truncated
+    green = factory(mat0.green_operator(), phase.shape, 1.0, dtype=dtype)
+    return phase, tens, green, np.eye(6)
+
+
+# ---------------------------------------------------------------------------
+# CPU leg: the reference's serial path (or the oracle port) on one load case
+# ---------------------------------------------------------------------------
+
+def reference_available():
+    from oracle import reference
+    return reference.load()
+
+
+def cpu_worker(n, seed, load, iters, variant, out_path):
+    """Run `iters` basic-scheme iterations of one load case with the
+    reference's own objects (the tutorial loop, square_basic.py:83-92)."""
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    import numpy as np
+    from janus_b200 import microstructures as micro
+    phase, _ = micro.random_spheres(n, radius=8 * n / 128, volume_fraction=0.3, seed=seed)
+    E = np.zeros(6)
+    E[load] = 1.0
+    ref = reference_available()
+    times = []
+    if ref is not None:
+        kind = "reference"
+        import janus.fft.serial as rfft
+        import janus.green as rgreen
+        import janus.material.elastic.linear.isotropic as rmat
+        import janus.operators as rops
+        mat0 = rmat.create(*REF_MEDIUM, 3)
+        tens = []
+        for g, nu in (MATRIX, INCLUSION):
+            m = rmat.create(g, nu, 3)
+            tens.append(rops.isotropic_4(3 * (m.k - mat0.k), 2 * (m.g - mat0.g), 3))
+        loc_arr = np.empty(phase.shape, dtype=object)
+        loc_arr[phase == 0] = tens[0]
+        loc_arr[phase == 1] = tens[1]
+        loc = rops.block_diagonal_operator(loc_arr)
+        fac = rgreen.filtered if variant == "filtered" else rgreen.truncated
+        green = fac(mat0.green_operator(), phase.shape, 1.0, rfft.create_real(phase.shape))
+        eps = np.empty(phase.shape + (6,))
+        eps[...] = E
+        new = np.empty_like(eps)
+        norm = 1 / np.sqrt(eps[..., 0].size) / np.linalg.norm(E)
+        for _ in range(iters):
+            t0 = time.perf_counter()
+            loc.apply(eps, new)
+            green.apply(new, new)
+            np.subtract(E, new, out=new)
+            _ = norm * np.linalg.norm(new - eps)
+            eps, new = new, eps
+            times.append(time.perf_counter() - t0)
+    else:
+        kind = "port"
+        from oracle import janus_oracle as O
+        pars = [O.delta_c(*MATRIX, *REF_MEDIUM, 3), O.delta_c(*INCLUSION, *REF_MEDIUM, 3)]
+        G = O.spectral_green_field(phase.shape, 1.0, *REF_MEDIUM, variant)
+        eps = np.empty(phase.shape + (6,))
+        eps[...] = E
+        for _ in range(iters):
+            t0 = time.perf_counter()
+            tau = O.phase_apply(eps, phase, [p[0] for p in pars], [p[1] for p in pars], 3)
+            y = O.green_apply(tau, *REF_MEDIUM, 1.0, variant, G=G)
+            new = E - y
+            _ = np.linalg.norm(new - eps)
+            eps = new
+            times.append(time.perf_counter() - t0)
+    with open(out_path, "w") as f:
+        json.dump({"kind": kind, "times": times}, f)
+
+
+def run_cpu_workers(n, seed, loads, iters, variant, tag):
+    import tempfile
+    procs = []
+    outs = []
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1",
+               MKL_NUM_THREADS="1", CUDA_VISIBLE_DEVICES="")
+    tmpdir = tempfile.mkdtemp(prefix="jb_cpu_")
+    for load in loads:
+        out = os.path.join(tmpdir, f"{tag}_{load}.json")
+        outs.append(out)
+        procs.append(subprocess.Popen(
+            [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--n", str(n),
+             "--seed", str(seed), "--load", str(load), "--iters", str(iters),
+             "--variant", variant, "--out", out], env=env))
+    for p in procs:
+        p.wait()
+    results = []
+    for p, out in zip(procs, outs):
+        if p.returncode != 0 or not os.path.exists(out):
+            raise RuntimeError("CPU worker failed")
+        with open(out) as f:
+            results.append(json.load(f))
+    return results
+
+
+def cpu_baseline(n, seed, variant, budget_s=20.0):
+    """1-core time of the reference's serial path on one load case:
+    iterations until about `budget_s` of CPU work (at least 2)."""
+    probe = run_cpu_workers(n, seed, [5], 2, variant, "probe")[0]
+    per_it = max(probe["times"][1], 1e-3)
+    iters = max(2, min(20, int(budget_s / per_it)))
+    res = run_cpu_workers(n, seed, [5], iters + 1, variant, "base")[0]
+    t = sum(res["times"][1:])
+    vox = n ** 3
+    return {"value": vox * iters / t, "unit": UNIT, "cores": 1, "kind": res["kind"],
+            "sample": f"{iters} basic-scheme iterations of one load case (E = xy) at {n}^3, "
+                      "after 1 untimed iteration, single thread"}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_gpu(args, rank, world, dist):
+    import numpy as np
+    import torch
+
+    from janus_b200 import operators as ops
+    from janus_b200.solvers import BasicScheme
+
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dtype = torch.float64 if args.dtype == "f64" else torch.float32
+    n = args.n
+    phase, tens, green, E = build_problem(n, 2024 + rank, args.variant, dtype)
+    loc = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dtype)
+    solver = BasicScheme(green, loc, nload=6)
+    solver.set_load(E)
+    eps = solver.new_field()
+    eps[...] = torch.from_numpy(E).to(dtype).cuda().view(6, 1, 1, 1, 6)
+    res = torch.zeros(6, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        solver.step(eps, res)
+    torch.cuda.synchronize()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    gpu_index = vis.split(",")[local] if vis else str(local)
+    sampler = ClockSampler(gpu_index)
+    sampler.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    solver.timing_begin(args.steps)
+    start.record()
+    for _ in range(args.steps):
+        solver.step(eps, res)
+    end.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    passes, nrec = solver.timing_end()
+    clocks = sampler.stop()
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    vox_step = 6 * n ** 3
+    value = world * vox_step * args.steps / (ms / 1e3)
+
+    # roofline of the dominant pass (algorithmic bytes / its mean duration)
+    p = 8 if dtype == torch.float64 else 4
+    pbytes = pass_bytes(6, p)
+    dom = max(passes, key=lambda k: passes[k])
+    dom_ms = passes[dom] / max(nrec, 1)
+    peak, peak_kind = measured_peak()
+    bytes_launch = pbytes[dom] * vox_step
+    achieved = bytes_launch / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        key = f"{dom}@{n}^3x6/{args.variant}/{args.dtype}"
+        if key in tj:
+            traffic = tj[key]
+    step_bytes = sum(pbytes.values()) * vox_step
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_launch,
+                "step_achieved": round(step_bytes / (ms / args.steps / 1e3) / 1e9, 1),
+                "step_frac": round(step_bytes / (ms / args.steps / 1e3) / 1e9 / peak, 4)}
+
+    # end to end through the public API with host buffers: host phase map and
+    # E in, strain field out (pinned), K iterations with the per-iteration
+    # residual read back
+    e2e = None
+    if not args.no_e2e:
+        out = torch.empty(solver.field_shape, dtype=dtype, pin_memory=True)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        loc2 = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dtype)
+        r = BasicScheme(green, loc2, nload=6).run(E, args.steps)
+        out.copy_(r.eps, non_blocking=True)
+        s1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_ms = max(s0.elapsed_time(s1), wall * 1e3)
+        if dist is not None:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * vox_step * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int((phase.nbytes + E.nbytes) / args.steps),
+               "d2h_bytes_per_step": int((out.numel() * out.element_size()) / args.steps
+                                         + 6 * 8),
+               "what": "operators from a host phase map, basic_scheme() for K iterations "
+                       "(residuals read back every iteration), strain field copied to "
+                       "pinned host memory"}
+
+    solve = None
+    if not args.no_solve and rank == 0 and world == 1:
+        import janus_b200.material.elastic.linear.isotropic as material
+        eps2 = solver.new_field()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        rr = solver.run(E, args.solve_max_iter, tol=args.tol, eps=eps2, init=True)
+        b.record()
+        torch.cuda.synchronize()
+        solve = {"tol": args.tol, "iterations": rr.iterations,
+                 "seconds": round(a.elapsed_time(b) / 1e3, 4),
+                 "final_residual_max": float(rr.residuals[-1].max()),
+                 "C_eff_diag": [float(v) for v in np.diag(
+                     rr.mean_stress(material.create(*REF_MEDIUM, 3), E))]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(n, 2024, args.variant)
+        except Exception as exc:  # pragma: no cover
+            cpu = {"value": None, "unit": UNIT, "error": str(exc)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": f"3D two-phase random spheres {n}^3 (radius {8 * n // 128}, "
+                                   "vf 0.3, seeded RSA), mu 1/100, nu 0.3/0.2, mu0 50.5, "
+                                   f"{args.variant} Green operator, 6 load cases, basic scheme",
+                       "grid": [n, n, n], "load_cases": 6, "variant": args.variant,
+                       "precision": args.dtype, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (strain fields "
+                             f"{6 * n ** 3 * 6 * p / 1e6:.0f} MB per step)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": nrec * len(passes),
+            "passes_ms_per_step": {k: round(v / max(nrec, 1), 4) for k, v in passes.items()},
+            "clocks": clocks, "solve": solve,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    n = args.n
+    results = run_cpu_workers(n, 2024, list(range(6)), args.warmup + args.steps, args.variant,
+                              "ref")
+    kind = results[0]["kind"]
+    t = max(sum(r["times"][args.warmup:]) for r in results)
+    value = 6 * n ** 3 * args.steps / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3D two-phase random spheres {n}^3 (radius {8 * n // 128}, "
+                               "vf 0.3, seeded RSA), mu 1/100, nu 0.3/0.2, mu0 50.5, "
+                               f"{args.variant} Green operator, 6 load cases, basic scheme",
+                   "grid": [n, n, n], "load_cases": 6, "variant": args.variant,
+                   "precision": "f64", "parallelism": "6 single-threaded processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 6, "kind": kind,
+                         "sample": f"{args.steps} timed iterations (after {args.warmup}) of "
+                                   f"each of the 6 load cases at {n}^3, one process per load "
+                                   "case (the reference's serial path is single-threaded)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="janus_b200", choices=["janus_b200", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--variant", default="filtered", choices=["filtered", "truncated"])
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--solve-max-iter", type=int, default=3000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-solve", action="store_true")
+    # internal: CPU worker process
+    ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--seed", type=int, default=2024, help=argparse.SUPPRESS)
+    ap.add_argument("--load", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--iters", type=int, default=1, help=argparse.SUPPRESS)
+    ap.add_argument("--out", default=None, help=argparse.SUPPRESS)
+    args = ap.parse_args(argv)
+    if args.warmup < 0 or args.steps < 1:
+        ap.error("steps must be >= 1 and warmup >= 0")
+
+    if args.cpu_worker:
+        cpu_worker(args.n, args.seed, args.load, args.iters, args.variant, args.out)
+        return
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        run_gpu(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -165,6 +165,15 @@ int jb_solver_set_load(jb_solver *solver, const double *E);
  * double[nload], may be NULL). */
 int jb_solver_step(jb_solver *solver, void *eps, double *res_dev,
                    void *stream);
+/* Benchmark support: record CUDA events around every pass of the next
+ * `max_steps` calls of jb_solver_step (on their stream). */
+int jb_solver_timing_begin(jb_solver *solver, int max_steps);
+/* Wait for the recorded steps; pass_ms[i] = total device time of pass i
+ * (ms, summed over the steps; room for 8 passes), npass and nsteps out. */
+int jb_solver_timing_end(jb_solver *solver, double *pass_ms, int *npass,
+                         int *nsteps);
+/* Name of pass i of one solver step ("" if out of range). */
+const char *jb_solver_pass_name(jb_solver *solver, int i);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -65,6 +65,9 @@ _SIGS = {
                        P_double, c_void_p], c_int),
     "jb_solver_set_load": ([c_void_p, P_double], c_int),
     "jb_solver_step": ([c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+    "jb_solver_timing_begin": ([c_void_p, c_int], c_int),
+    "jb_solver_timing_end": ([c_void_p, P_double, P_int, P_int], c_int),
+    "jb_solver_pass_name": ([c_void_p, c_int], ctypes.c_char_p),
 }
 
 

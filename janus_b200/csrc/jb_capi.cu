@@ -256,6 +256,24 @@ struct jb_local_s {
   void* table = nullptr;
 };
 
+// CUDA events recorded between the passes of solver steps (benchmarks)
+struct PassRecorder {
+  std::vector<cudaEvent_t> ev;
+  int npass = 0;
+  int max_steps = 0;
+  int steps = 0;
+  size_t cursor = 0;
+  bool active = false;
+  void mark(cudaStream_t st) {
+    if (active && cursor < ev.size()) cudaEventRecord(ev[cursor++], st);
+  }
+  void release() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    ev.clear();
+    active = false;
+  }
+};
+
 struct jb_solver_s {
   jb_green* green = nullptr;
   jb_local* local = nullptr;
@@ -265,6 +283,7 @@ struct jb_solver_s {
   std::vector<double> norm;  // 1 / (sqrt(N) |E_l|)
   int nb_rows = 0;
   bool load_set = false;
+  PassRecorder rec;
 };
 
 namespace {
@@ -296,7 +315,9 @@ int upload_table(jb_green* g, int dtype, const std::vector<double>& v, void** ou
 // x: real fields (or eps with local), spec: complex scratch, y: output
 int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
                  const jb::LocalDesc* local, const jb::UpdateDesc* upd, int* nb_rows,
-                 cudaStream_t st) {
+                 cudaStream_t st, PassRecorder* rec = nullptr) {
+  PassRecorder dummy;
+  if (!rec) rec = &dummy;
   const int dim = g->dim;
   const int C = dim == 2 ? 3 : 6;
   const int64_t n0 = g->n[0], n1 = g->n[1], n2 = g->n[2];
@@ -320,23 +341,31 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
   }
   const AxisData& last = g->ax[dim - 1];
   if ((int64_t)L > 65535) return fail(JB_EINVAL, "batch too large (max 65535)");
+  rec->mark(st);
   JB_TRY(launch_status(jb::launch_rows_r2c(g->dtype, last, C, (int)L, x, geom, spec, local, st),
                        "rows_r2c"));
-  if (dim == 3)
+  rec->mark(st);
+  if (dim == 3) {
     JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 0, L * n0, m * C, spec, spec, C,
                                          dim, nullptr, n1, m, st),
                          "cols_fwd_axis1"));
+    rec->mark(st);
+  }
   const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
   JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
                                        &g->gt, n1, m, st),
                        "cols_green_axis0"));
-  if (dim == 3)
+  rec->mark(st);
+  if (dim == 3) {
     JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 1, L * n0, m * C, spec, spec, C,
                                          dim, nullptr, n1, m, st),
                          "cols_inv_axis1"));
+    rec->mark(st);
+  }
   JB_TRY(launch_status(jb::launch_rows_c2r(g->dtype, last, C, (int)L, spec, y, geom,
                                            1.0 / (double)N, upd, nb_rows, st),
                        "rows_c2r"));
+  rec->mark(st);
   return JB_OK;
 }
 
@@ -819,6 +848,7 @@ int jb_solver_create(jb_green* G, jb_local* L, int nload, jb_solver** out) {
 
 int jb_solver_destroy(jb_solver* S) {
   if (!S) return JB_OK;
+  S->rec.release();
   for (DeviceBuf* b : {&S->spec, &S->partials, &S->E, &S->res, &S->mean, &S->normd})
     if (b->p) cudaFree(b->p);
   delete S;
@@ -854,15 +884,67 @@ int jb_solver_step(jb_solver* S, void* eps, double* res_dev, void* stream) {
   upd.E = static_cast<const double*>(S->E.p);
   upd.partials = static_cast<double*>(S->partials.p);
   int nb = 0;
-  JB_TRY(green_passes(S->green, eps, eps, S->L, S->spec.p, &loc, &upd, &nb, st));
+  PassRecorder* rec = nullptr;
+  if (S->rec.active && S->rec.steps < S->rec.max_steps) {
+    rec = &S->rec;
+    ++S->rec.steps;
+  }
+  JB_TRY(green_passes(S->green, eps, eps, S->L, S->spec.p, &loc, &upd, &nb, st, rec));
   if (res_dev) {
     JB_TRY(launch_status(jb::launch_reduce_rows(static_cast<const double*>(S->partials.p), S->L,
                                                 nb, res_dev, 1.0,
                                                 static_cast<const double*>(S->normd.p), 1, st),
                          "reduce"));
   }
+  if (rec) rec->mark(st);
   S->nb_rows = nb;
   return JB_OK;
+}
+
+static const char* kPass3[] = {"rows_r2c_local", "cols_fwd_axis1", "cols_green_axis0",
+                               "cols_inv_axis1", "rows_c2r_update", "reduce_residual"};
+static const char* kPass2[] = {"rows_r2c_local", "cols_green_axis0", "rows_c2r_update",
+                               "reduce_residual"};
+
+int jb_solver_timing_begin(jb_solver* S, int max_steps) {
+  if (!S) return fail(JB_EINVAL, "NULL argument");
+  if (max_steps < 1) return fail(JB_EINVAL, "max_steps must be >= 1");
+  S->rec.release();
+  S->rec.npass = S->green->dim == 3 ? 6 : 4;
+  S->rec.max_steps = max_steps;
+  S->rec.steps = 0;
+  S->rec.cursor = 0;
+  S->rec.ev.resize((size_t)(S->rec.npass + 1) * max_steps);
+  for (auto& e : S->rec.ev) JB_CUDA(cudaEventCreate(&e));
+  S->rec.active = true;
+  return JB_OK;
+}
+
+int jb_solver_timing_end(jb_solver* S, double* pass_ms, int* npass, int* nsteps) {
+  if (!S || !pass_ms) return fail(JB_EINVAL, "NULL argument");
+  PassRecorder& R = S->rec;
+  if (!R.active) return fail(JB_ESTATE, "jb_solver_timing_begin was not called");
+  const int P = R.npass;
+  for (int i = 0; i < 8; ++i) pass_ms[i] = 0.0;
+  const int done = (int)(R.cursor / (P + 1));
+  if (R.cursor > 0) JB_CUDA(cudaEventSynchronize(R.ev[R.cursor - 1]));
+  for (int s = 0; s < done; ++s)
+    for (int p = 0; p < P; ++p) {
+      float ms = 0.f;
+      JB_CUDA(cudaEventElapsedTime(&ms, R.ev[(size_t)s * (P + 1) + p],
+                                   R.ev[(size_t)s * (P + 1) + p + 1]));
+      pass_ms[p] += ms;
+    }
+  if (npass) *npass = P;
+  if (nsteps) *nsteps = done;
+  R.release();
+  return JB_OK;
+}
+
+const char* jb_solver_pass_name(jb_solver* S, int i) {
+  if (!S || i < 0) return "";
+  if (S->green->dim == 3) return i < 6 ? kPass3[i] : "";
+  return i < 4 ? kPass2[i] : "";
 }
 
 int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_iter, double tol,

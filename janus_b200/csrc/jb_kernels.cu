@@ -403,15 +403,25 @@ __global__ void reduce_rows_kernel(const double* partials, int nb, double* out, 
 std::mutex g_attr_mu;
 std::unordered_map<const void*, size_t> g_attr;
 
+// Opt the kernel in to `bytes` of dynamic shared memory (static + dynamic
+// must stay within the 227 KB per-block limit).
 cudaError_t ensure_smem(const void* fn, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
   std::lock_guard<std::mutex> lk(g_attr_mu);
   auto it = g_attr.find(fn);
   if (it != g_attr.end() && it->second >= bytes) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kSmemCap);
-  if (e == cudaSuccess) g_attr[fn] = kSmemCap;
-  return e;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  const size_t cap = kSmemCap - fa.sharedSizeBytes;
+  if (bytes > cap) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // do not leave the failure behind for later launches
+    return e;
+  }
+  g_attr[fn] = cap;
+  return cudaSuccess;
 }
 
 int grid_for(int64_t total) {

@@ -121,6 +121,22 @@ class BasicScheme:
         _lib.check(_lib.lib().jb_solver_set_load(
             self._handle, E.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
 
+    def timing_begin(self, max_steps):
+        """Record CUDA events around each pass of the next max_steps steps."""
+        _lib.check(_lib.lib().jb_solver_timing_begin(self._handle, int(max_steps)))
+
+    def timing_end(self):
+        """{pass name: total device ms} over the recorded steps, and the
+        number of steps recorded."""
+        ms = (ctypes.c_double * 8)()
+        npass = ctypes.c_int(0)
+        nsteps = ctypes.c_int(0)
+        _lib.check(_lib.lib().jb_solver_timing_end(self._handle, ms, ctypes.byref(npass),
+                                                   ctypes.byref(nsteps)))
+        names = [_lib.lib().jb_solver_pass_name(self._handle, i).decode()
+                 for i in range(npass.value)]
+        return {n: ms[i] for i, n in enumerate(names)}, nsteps.value
+
     def step(self, eps, res_dev=None):
         """One asynchronous iteration on the current stream (after set_load)."""
         _lib.check(_lib.lib().jb_solver_step(

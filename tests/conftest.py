@@ -52,19 +52,5 @@ def golden_cases(data):
 def reference_checker():
     """The reference's Cython modules built against the FFT shim, if built
     (oracle/_ref); None otherwise."""
-    path = os.path.join(ROOT, "oracle", "_ref")
-    if not os.path.isdir(os.path.join(path, "janus")):
-        return None
-    if path not in sys.path:
-        sys.path.insert(0, path)
-    try:
-        import janus.green  # noqa: F401
-        import janus.fft.serial  # noqa: F401
-        import janus.material.elastic.linear.isotropic  # noqa: F401
-        import janus.operators  # noqa: F401
-    except Exception:
-        return None
-    import janus
-    if "oracle" not in (getattr(janus, "__file__", "") or ""):
-        return None
-    return janus
+    from oracle import reference
+    return reference.load()
