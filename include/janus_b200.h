@@ -106,6 +106,22 @@ int jb_green_destroy(jb_green *green);
  * of `batch` contiguous fields; x == y is allowed. */
 int jb_green_apply(jb_green *green, const void *x, void *y, int64_t batch,
                    void *stream);
+/* No counterpart in the reference.  y = Gamma0[x] (FP64, one field, x == y
+ * allowed) for callers that cannot allocate device memory at all: code under
+ * an allocator that owns the whole GPU, a host application that forbids
+ * cudaMalloc/cudaFree outside its set-up phase, or a plug-in that is handed
+ * only its input and output buffers.  It takes no handle and allocates
+ * nothing: twiddles, Green tables and the spectral scratch live in one
+ * 32 MiB file-scope device array that every GPU loading this library holds
+ * until exit.  Limit: the half spectrum n0*(n1)*(n_last/2+1)*s*16 bytes must
+ * fit in 31 MiB (FP64 2D up to about 1024 x 1024, 3D up to about 80^3) and
+ * no axis may exceed 4096; larger grids get JB_EINVAL with the size in the
+ * message.  The first call on a device (with that device current) looks up
+ * the array's address, so make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race. */
+int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
+                           double nu, int variant, const double *x, double *y,
+                           void *stream);
 /* set_frequency + to_memoryview at index b (green.pyx:146-171, 312-342 and
  * the subclasses' c_set_frequency / c_to_memoryview): host, FP64, with the
  * reference's range checks (0 <= b_i < n_i). */

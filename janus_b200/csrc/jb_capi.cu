@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -995,3 +996,145 @@ int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_it
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Green operator application without any device allocation
+// ===========================================================================
+//
+// For callers that cannot allocate device memory at all: code running under
+// an allocator that owns the whole GPU (a memory pool sized at start-up), a
+// host application that forbids cudaMalloc/cudaFree outside its set-up phase,
+// or a plug-in whose host framework hands it only input and output buffers.
+// jb_green_apply_noalloc needs no handle: the twiddle tables, the Green
+// operator's k/weight tables and the spectral scratch all live in the one
+// file-scope device array below (32 MiB, held by every GPU that loads this
+// library until the process exits).
+//
+// Set-up: the first call on a device, with that device current, looks up the
+// array's device address (cudaGetSymbolAddress) and caches it per device, so
+// make the first call on each device before any stream capture.  The array
+// keeps the last call's contents; nothing in it needs to start at zero (every
+// region is written before it is read within a call).  Calls share the
+// array, so two calls that overlap on the GPU (different streams, or
+// different host threads without ordering) race.
+namespace {
+
+constexpr size_t kNoAllocBytes = size_t(32) << 20;       // whole array
+constexpr size_t kNoAllocTwOff = 0;                      // 3 x 64 KiB twiddles
+constexpr size_t kNoAllocTwBytes = size_t(64) << 10;
+constexpr size_t kNoAllocTabOff = size_t(192) << 10;     // 3 axes x 4 tables
+constexpr size_t kNoAllocTabBytes = size_t(4096) * 8;    // per table
+constexpr size_t kNoAllocSpecOff = size_t(1) << 20;      // spectral scratch
+constexpr int kNoAllocMaxAxis = 4096;
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  JB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(JB_EINVAL, "jb_green_apply_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return fail(JB_ECUDA, std::string("jb_green_apply_noalloc: cudaGetSymbolAddress: ") +
+                                cudaGetErrorString(e));
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return JB_OK;
+}
+
+}  // namespace
+
+extern "C" int jb_green_apply_noalloc(int dim, const int64_t* shape, double h, double g,
+                                      double nu, int variant, const double* x, double* y,
+                                      void* stream) {
+  if (!x || !y) return fail(JB_EINVAL, "NULL argument");
+  JB_TRY(check_shape(dim, shape, F64));
+  if (!(h > 0.)) return fail(JB_EINVAL, "h must be > 0 (was " + std::to_string(h) + ")");
+  if (variant != JB_TRUNCATED && variant != JB_FILTERED)
+    return fail(JB_EINVAL, "variant must be JB_TRUNCATED or JB_FILTERED");
+  for (int d = 0; d < dim; ++d)
+    if (shape[d] > kNoAllocMaxAxis)
+      return fail(JB_EINVAL, "jb_green_apply_noalloc: axis longer than 4096");
+  const int C = dim == 2 ? 3 : 6;
+  const int64_t nlast = shape[dim - 1];
+  const int64_t rows = dim == 2 ? shape[0] : shape[0] * shape[1];
+  const size_t need = (size_t)rows * (nlast / 2 + 1) * C * 16;
+  if (need > kNoAllocBytes - kNoAllocSpecOff)
+    return fail(JB_EINVAL, "jb_green_apply_noalloc: this grid needs " + std::to_string(need) +
+                               " bytes of spectral scratch; the static scratch holds " +
+                               std::to_string(kNoAllocBytes - kNoAllocSpecOff) +
+                               " (FP64: 2D up to about 1024 x 1024, 3D up to about 80^3)");
+  void* base = nullptr;
+  JB_TRY(noalloc_scratch(&base));
+  unsigned char* b8 = static_cast<unsigned char*>(base);
+  cudaStream_t st = as_stream(stream);
+
+  // a stack-held operator description whose device pointers all point into
+  // the static array (no handle, no allocation)
+  jb_green G;
+  G.dim = dim;
+  G.dtype = F64;
+  G.variant = variant;
+  G.h = h;
+  G.g = g;
+  G.nu = nu;
+  G.gt.variant = variant;
+  G.gt.inv2g = 0.5 / g;
+  G.gt.c1 = 1.0 / (1.0 - nu);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  std::vector<double> tw, tab[4];
+  for (int d = 0; d < dim; ++d) {
+    const int64_t n = shape[d];
+    G.n[d] = n;
+    G.s[d] = 2. * M_PI / (h * (double)n);
+    factorize((int)n, G.ax[d].plan);
+    tw.resize(2 * (size_t)n);
+    for (int64_t t = 0; t < n; ++t) {
+      long double a = two_pi * (long double)t / (long double)n;
+      tw[2 * t] = (double)cosl(a);
+      tw[2 * t + 1] = (double)-sinl(a);
+    }
+    G.ax[d].tw = b8 + kNoAllocTwOff + d * kNoAllocTwBytes;
+    JB_CUDA(cudaMemcpyAsync(G.ax[d].tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice, st));
+    const double sd = G.s[d];
+    for (auto& v : tab) v.assign(n, 0.0);
+    for (int64_t b = 0; b < n; ++b) {
+      if (variant == JB_TRUNCATED) {
+        tab[0][b] = 2 * b > n ? sd * (b - n) : sd * b;
+      } else {
+        double k = sd * (b - n);
+        double w = cos(0.25 * h * k);
+        w *= w;
+        tab[0][b] = k;
+        tab[2][b] = w;
+        k = sd * b;
+        w = cos(0.25 * h * k);
+        w *= w;
+        tab[1][b] = k;
+        tab[3][b] = w;
+      }
+    }
+    void** slots[4] = {variant == JB_TRUNCATED ? &G.gt.kt[d] : &G.gt.kn[d], &G.gt.kp[d],
+                       &G.gt.wn[d], &G.gt.wp[d]};
+    const int ntab = variant == JB_TRUNCATED ? 1 : 4;
+    for (int i = 0; i < ntab; ++i) {
+      void* dst = b8 + kNoAllocTabOff + (size_t)(d * 4 + i) * kNoAllocTabBytes;
+      JB_CUDA(cudaMemcpyAsync(dst, tab[i].data(), n * 8, cudaMemcpyHostToDevice, st));
+      *slots[i] = dst;
+    }
+  }
+  const int r = green_passes(&G, x, y, 1, b8 + kNoAllocSpecOff, nullptr, nullptr, nullptr, st);
+  for (int d = 0; d < 3; ++d) G.ax[d].tw = nullptr;  // not owned
+  return r;
+}
