@@ -56,6 +56,11 @@ int jb_version(void);
 const char *jb_last_error(void);
 /* Largest supported length of one grid axis for a precision. */
 int jb_max_axis_length(int dtype);
+/* Device-side fault word of the current device, read and cleared: bit 0 set
+ * means a kernel gave up a bounded wait on its own asynchronous copies and
+ * skipped its tile (no reference counterpart; the reference has no device
+ * code).  Synchronises with the device. */
+int jb_device_status(unsigned *fault);
 
 /* ---- real FFT objects ------------------------------------------------- */
 

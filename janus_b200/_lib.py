@@ -37,6 +37,7 @@ _SIGS = {
     "jb_version": ([], c_int),
     "jb_last_error": ([], ctypes.c_char_p),
     "jb_max_axis_length": ([c_int], c_int),
+    "jb_device_status": ([ctypes.POINTER(ctypes.c_uint)], c_int),
     "jb_fft_create": ([c_int, P_int64, c_int, ctypes.c_uint, ctypes.POINTER(c_void_p)], c_int),
     "jb_fft_destroy": ([c_void_p], c_int),
     "jb_fft_r2c": ([c_void_p, c_void_p, P_int64, c_void_p, c_void_p], c_int),
@@ -101,6 +102,13 @@ def check(status: int) -> None:
     if status == JB_EINVAL:
         raise ValueError(msg)
     raise RuntimeError(f"janus_b200 native call failed ({status}): {msg}")
+
+
+def device_status() -> int:
+    """Read and clear the device fault word (bit 0: a bounded wait gave up)."""
+    v = ctypes.c_uint(0)
+    check(lib().jb_device_status(ctypes.byref(v)))
+    return v.value
 
 
 def i64_array(values):

@@ -57,6 +57,13 @@ void factorize(int n, jb::AxisPlan& p) {
   for (int f = 7; m > 1 && (long)f * f <= m; f += 2)
     while (m % f == 0) { p.fac[p.nf++] = f; m /= f; }
   if (m > 1) p.fac[p.nf++] = m;
+  int Ns = 1;
+  for (int f = 0; f < p.nf; ++f) {
+    p.tstep[f] = n / (Ns * p.fac[f]);
+    // ceil(2^32 / Ns): q = umulhi(j, magic) == j / Ns for j < 2^16
+    p.nsmagic[f] = Ns > 1 ? (unsigned)((((uint64_t)1 << 32) + Ns - 1) / Ns) : 0u;
+    Ns *= p.fac[f];
+  }
 }
 
 struct DeviceBuf {
@@ -386,6 +393,12 @@ int jb_version(void) { return 100; }
 const char* jb_last_error(void) { return g_err.c_str(); }
 
 int jb_max_axis_length(int dtype) { return jb::max_axis_length(dtype); }
+
+int jb_device_status(unsigned* fault) {
+  if (!fault) return fail(JB_EINVAL, "NULL argument");
+  JB_CUDA(jb::read_and_clear_fault(fault));
+  return JB_OK;
+}
 
 // ---------------------------------------------------------------------------
 // FFT

@@ -136,28 +136,55 @@ template <int DIR, typename C> struct Dft<8, DIR, C> {
 // ---------------------------------------------------------------------------
 // one Stockham stage over a W-column tile
 // ---------------------------------------------------------------------------
+//
+// Thread mapping: a block of T*W threads; thread t works on column
+// t % W and on the butterflies j = t / W, t / W + T, ... of every stage, so
+// the inner loops need no integer division.  k = j mod Ns uses a
+// multiply-high by the host-computed ceil(2^32 / Ns), exact for j < 2^16.
+
+struct AxisPlan {
+  int n;
+  int nf;
+  int fac[24];
+  int tstep[24];          // n / (Ns_f * R_f): twiddle index step of stage f
+  unsigned nsmagic[24];   // ceil(2^32 / Ns_f) (0 when Ns_f == 1)
+};
+
+struct Lane {
+  int col;  // column of the tile
+  int j0;   // first butterfly
+  int T;    // butterfly stride (threads per column)
+};
+
+__device__ __forceinline__ Lane make_lane(int W) {
+  Lane l;
+  l.T = blockDim.x / W;
+  l.col = threadIdx.x % W;
+  l.j0 = threadIdx.x / W;
+  if (l.j0 >= l.T) l.j0 = 1 << 30;  // surplus threads take no butterflies
+  return l;
+}
+
 template <int R, int DIR, typename C>
 __device__ __forceinline__ void stage_fixed(const C* __restrict__ x, C* __restrict__ y,
                                             const C* __restrict__ tw, int n, int Ns,
-                                            int W) {
+                                            unsigned magic, int tstep, int W, Lane ln) {
   const int nr = n / R;
-  const int tstep = n / (Ns * R);
-  const int nb = nr * W;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    const int j = b / W;
-    const int col = b - j * W;
-    const int k = j % Ns;
+  for (int j = ln.j0; j < nr; j += ln.T) {
+    const int q = Ns == 1 ? j : (int)__umulhi((unsigned)j, magic);
+    const int k = j - q * Ns;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = x[(j + r * nr) * W + col];
+    for (int r = 0; r < R; ++r) v[r] = x[(j + r * nr) * W + ln.col];
     if (k != 0) {
+      const int kt = k * tstep;
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<DIR>(tw, k * r * tstep));
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<DIR>(tw, kt * r));
     }
     Dft<R, DIR, C>::run(v);
-    const int base = (j - k) * R + k;
+    const int base = q * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) y[(base + r * Ns) * W + col] = v[r];
+    for (int r = 0; r < R; ++r) y[(base + r * Ns) * W + ln.col] = v[r];
   }
 }
 
@@ -166,52 +193,46 @@ __device__ __forceinline__ void stage_fixed(const C* __restrict__ x, C* __restri
 template <int DIR, typename C>
 __device__ __forceinline__ void stage_generic(const C* __restrict__ x, C* __restrict__ y,
                                               const C* __restrict__ tw, int n, int Ns,
-                                              int W, int R) {
+                                              unsigned magic, int tstep, int W, int R,
+                                              Lane ln) {
   using T = decltype(x[0].x);
   const int nr = n / R;
-  const int tstep = n / (Ns * R);
-  const int nb = nr * W;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    const int j = b / W;
-    const int col = b - j * W;
-    const int k = j % Ns;
-    const int base = (j - k) * R + k;
+  for (int j = ln.j0; j < nr; j += ln.T) {
+    const int q0 = Ns == 1 ? j : (int)__umulhi((unsigned)j, magic);
+    const int k = j - q0 * Ns;
+    const int base = q0 * Ns * R + k;
     for (int q = 0; q < R; ++q) {
       C acc = mkc(T(0), T(0));
       for (int r = 0; r < R; ++r) {
-        C v = x[(j + r * nr) * W + col];
+        C v = x[(j + r * nr) * W + ln.col];
         if (k != 0 && r != 0) v = cmul(v, twid<DIR>(tw, k * r * tstep));
         const int t = ((r * q) % R) * nr;  // w_R^(rq) = w_n^((rq mod R) n/R)
         acc = cadd(acc, cmul(v, twid<DIR>(tw, t)));
       }
-      y[(base + q * Ns) * W + col] = acc;
+      y[(base + q * Ns) * W + ln.col] = acc;
     }
   }
 }
-
-struct AxisPlan {
-  int n;
-  int nf;
-  int fac[24];
-};
 
 // Full 1D transform of all W columns of tile `a` (length n), using `b` as the
 // ping-pong partner.  Returns the tile that holds the result.  All threads of
 // the block must call it; it synchronises between stages.
 template <int DIR, typename C>
-__device__ C* fft_tile(C* a, C* b, const C* tw, const AxisPlan& p, int W) {
+__device__ C* fft_tile(C* a, C* b, const C* tw, const AxisPlan& p, int W, Lane ln) {
   int Ns = 1;
   C* x = a;
   C* y = b;
   for (int f = 0; f < p.nf; ++f) {
     const int R = p.fac[f];
+    const unsigned mg = p.nsmagic[f];
+    const int ts = p.tstep[f];
     switch (R) {
-      case 2: stage_fixed<2, DIR>(x, y, tw, p.n, Ns, W); break;
-      case 3: stage_fixed<3, DIR>(x, y, tw, p.n, Ns, W); break;
-      case 4: stage_fixed<4, DIR>(x, y, tw, p.n, Ns, W); break;
-      case 5: stage_fixed<5, DIR>(x, y, tw, p.n, Ns, W); break;
-      case 8: stage_fixed<8, DIR>(x, y, tw, p.n, Ns, W); break;
-      default: stage_generic<DIR>(x, y, tw, p.n, Ns, W, R); break;
+      case 2: stage_fixed<2, DIR>(x, y, tw, p.n, Ns, mg, ts, W, ln); break;
+      case 3: stage_fixed<3, DIR>(x, y, tw, p.n, Ns, mg, ts, W, ln); break;
+      case 4: stage_fixed<4, DIR>(x, y, tw, p.n, Ns, mg, ts, W, ln); break;
+      case 5: stage_fixed<5, DIR>(x, y, tw, p.n, Ns, mg, ts, W, ln); break;
+      case 8: stage_fixed<8, DIR>(x, y, tw, p.n, Ns, mg, ts, W, ln); break;
+      default: stage_generic<DIR>(x, y, tw, p.n, Ns, mg, ts, W, R, ln); break;
     }
     __syncthreads();
     Ns *= R;

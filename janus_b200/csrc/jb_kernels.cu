@@ -15,6 +15,7 @@
 #include <mutex>
 #include <unordered_map>
 
+#include "jb_async.cuh"
 #include "jb_green.cuh"
 #include "jb_kernels.h"
 
@@ -89,7 +90,8 @@ template <typename T> struct RowsArgs {
   const cx<T>* tw;
   AxisPlan plan;
   RealGeom g;
-  int C, R, W, m;
+  int R, W, m;
+  int contig;  // real side rows are contiguous [rows][n][C]
   int64_t cstride_l;
   const void* phase;
   int index_bytes;
@@ -104,129 +106,241 @@ __device__ __forceinline__ int64_t geom_off(const RealGeom& g, int64_t row, int 
   return (row / g.n1r) * g.s0 + (row % g.n1r) * g.s1 + e * g.es + c * g.cs;
 }
 
-template <typename T, bool LOCAL>
+template <typename P> __device__ __forceinline__ P* align16_ptr(void* p) {
+  return reinterpret_cast<P*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+}
+
+// every thread waits (bounded) on the tile barrier; false if any timed out
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, int* fail_flag) {
+  if (!mbar_wait(bar, 0)) atomicOr(fail_flag, 1);
+  __syncthreads();
+  return *fail_flag == 0;
+}
+
+// r2c along the contiguous axis of CC-component real rows, optionally with
+// the local operator (C - C0):eps fused on the way in.
+// Shared memory: twiddles | tile A | tile B, tiles (n+2) x W complex.
+//  1. the R-row input chunk (contiguous) lands in B by one bulk copy;
+//  2. B -> A transposes it so tile rows are the transform axis (real view:
+//     row e holds the R*CC reals of voxel e of each row), applying the local
+//     operator per voxel;
+//  3. Stockham FFT of the W complex columns (real columns paired as re/im);
+//  4. split into the two half spectra, staged as [rr][k][c] and written out
+//     by one bulk copy.
+template <typename T, int CC, bool LOCAL>
 __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int n = a.plan.n, W = a.W, R = a.R, Cc = a.C, m = a.m;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int fail_flag;
+  const int n = a.plan.n, W = a.W, R = a.R, m = a.m;
   C* tw = reinterpret_cast<C*>(smem);
-  C* A = tw + n;
-  C* B = A + (size_t)(n + 2) * W;
+  C* A = align16_ptr<C>(tw + n);
+  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
   T* Ar = reinterpret_cast<T*>(A);
+  T* Br = reinterpret_cast<T*>(B);
   const int ldr = 2 * W;
   const int l = blockIdx.y;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
-  const int RC = R * Cc;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  constexpr int kC = CC;
+  const int RC = R * kC;
   const T* xl = a.x + l * a.g.ls;
-  const int total = RC * n;
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int c = idx % Cc;
-    const int t = idx / Cc;
-    const int e = t % n;
-    const int rr = t / n;
-    T v = T(0);
-    if (rr < rows_here) v = xl[geom_off(a.g, row0 + rr, e, c)];
-    Ar[e * ldr + rr * Cc + c] = v;
+  const T* chunk = xl + row0 * n * kC;
+  const uint32_t bytes = (uint32_t)(rows_here * n * kC * sizeof(T));
+  const bool bulk = a.contig && aligned16(chunk) && (bytes % 16 == 0) && aligned16(Br);
+  if (threadIdx.x == 0) {
+    fail_flag = 0;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
+  __syncthreads();
+  if (bulk) {
+    if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, bytes);
+      bulk_load(Br, chunk, bytes, &bar);
+    }
+  } else {
+    for (int rr = 0; rr < rows_here; ++rr)
+      for (int e = threadIdx.x; e < n; e += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < kC; ++c)
+          Br[(rr * n + e) * kC + c] = xl[geom_off(a.g, row0 + rr, e, c)];
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  if (bulk) {
+    if (!tile_wait(&bar, &fail_flag)) return;
+  } else {
+    __syncthreads();
+  }
+  for (int rr = 0; rr < R; ++rr)
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      T v[kC];
+      if (rr < rows_here) {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[c] = Br[(rr * n + e) * kC + c];
+        if constexpr (LOCAL) {
+          const int ph = load_phase(a.phase, a.index_bytes, (row0 + rr) * n + e);
+          iso_apply<T>(v, a.table[2 * ph], a.table[2 * ph + 1], kC == 3 ? 2 : 3);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[c] = T(0);
+      }
+#pragma unroll
+      for (int c = 0; c < kC; ++c) Ar[e * ldr + rr * kC + c] = v[c];
+    }
   if (ldr > RC)
     for (int e = threadIdx.x; e < n; e += blockDim.x)
       for (int j = RC; j < ldr; ++j) Ar[e * ldr + j] = T(0);
   __syncthreads();
-  if (LOCAL) {
-    for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
-      const int e = idx % n;
-      const int rr = idx / n;
-      if (rr < rows_here) {
-        const int ph = load_phase(a.phase, a.index_bytes, (row0 + rr) * n + e);
-        iso_apply<T>(Ar + e * ldr + rr * Cc, a.table[2 * ph], a.table[2 * ph + 1], a.dim);
-      }
-    }
-    __syncthreads();
-  }
-  C* Z = fft_tile<-1>(A, B, tw, a.plan, W);
+  const Lane ln = make_lane(W);
+  C* Z = fft_tile<-1>(A, B, tw, a.plan, W, ln);
   C* S = (Z == A) ? B : A;
-  for (int idx = threadIdx.x; idx < m * W; idx += blockDim.x) {
-    const int col = idx % W;
-    const int k = idx / W;
-    const C P = Z[k * W + col];
-    const C Q = cconj(Z[(k == 0 ? 0 : n - k) * W + col]);
+  {
+    const int col = ln.col;
     const int ra = 2 * col, rb = 2 * col + 1;
-    const int rra = ra / Cc, ca = ra - rra * Cc;
-    const int rrb = rb / Cc, cb = rb - rrb * Cc;
-    if (ra < RC && rra < rows_here)
-      S[((int64_t)rra * m + k) * Cc + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
-    if (rb < RC && rrb < rows_here)
-      S[((int64_t)rrb * m + k) * Cc + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
+    const int rra = ra / kC, ca = ra - rra * kC;
+    const int rrb = rb / kC, cb = rb - rrb * kC;
+    for (int k = ln.j0; k < m; k += ln.T) {
+      const C P = Z[k * W + col];
+      const C Q = cconj(Z[(k == 0 ? 0 : n - k) * W + col]);
+      if (ra < RC && rra < rows_here)
+        S[((int64_t)rra * m + k) * kC + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
+      if (rb < RC && rrb < rows_here)
+        S[((int64_t)rrb * m + k) * kC + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
+    }
   }
+  fence_async_shared();
   __syncthreads();
-  C* dst = a.out + l * a.cstride_l + row0 * m * Cc;
-  const int cnt = rows_here * m * Cc;
-  for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) dst[idx] = S[idx];
+  C* dst = a.out + l * a.cstride_l + row0 * m * kC;
+  const uint32_t obytes = (uint32_t)(rows_here * m * kC * sizeof(C));
+  if (aligned16(dst) && obytes % 16 == 0) {
+    if (threadIdx.x == 0) {
+      bulk_store(dst, S, obytes);
+      bulk_commit();
+      bulk_wait_read();
+    }
+  } else {
+    const int cnt = rows_here * m * kC;
+    for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) dst[idx] = S[idx];
+  }
 }
 
-template <typename T, bool UPDATE>
+// c2r along the contiguous axis; the spectral chunk (and, for the solver
+// update, the old strain chunk) arrive by bulk copies; the output chunk
+// leaves by one bulk copy.  UPDATE: eps <- E - scale * y in place with FP64
+// residual partials (sum of squared increments) per block.
+template <typename T, int CC, bool UPDATE>
 __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int fail_flag;
   __shared__ double red[kThreads / 32];
-  const int n = a.plan.n, W = a.W, R = a.R, Cc = a.C, m = a.m;
+  constexpr int kC = CC;
+  const int n = a.plan.n, W = a.W, R = a.R, m = a.m;
   C* tw = reinterpret_cast<C*>(smem);
-  C* A = tw + n;
-  C* B = A + (size_t)(n + 2) * W;
+  C* A = align16_ptr<C>(tw + n);
+  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
+  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W);  // [R][n][CC] (UPDATE)
   const int ldr = 2 * W;
   const int l = blockIdx.y;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
-  const int RC = R * Cc;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
-  const C* src = a.cin + l * a.cstride_l + row0 * m * Cc;
-  const int cnt = rows_here * m * Cc;
-  for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) B[idx] = src[idx];
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
-    const int col = idx % W;
-    const int k = idx / W;
-    const int ra = 2 * col, rb = 2 * col + 1;
-    const int rra = ra / Cc, ca = ra - rra * Cc;
-    const int rrb = rb / Cc, cb = rb - rrb * Cc;
-    const bool mirror = 2 * k > n;
-    const int kk = mirror ? n - k : k;
-    C Av = mkc(T(0), T(0)), Bv = mkc(T(0), T(0));
-    if (ra < RC && rra < rows_here) Av = B[((int64_t)rra * m + kk) * Cc + ca];
-    if (rb < RC && rrb < rows_here) Bv = B[((int64_t)rrb * m + kk) * Cc + cb];
-    if (kk == 0 || 2 * kk == n) {
-      Av.y = T(0);
-      Bv.y = T(0);
-    }
-    A[k * W + col] = mirror ? mkc(Av.x + Bv.y, Bv.x - Av.y) : mkc(Av.x - Bv.y, Av.y + Bv.x);
+  const int RC = R * kC;
+  const C* src = a.cin + l * a.cstride_l + row0 * m * kC;
+  const uint32_t sbytes = (uint32_t)(rows_here * m * kC * sizeof(C));
+  T* yl = a.y + l * a.g.ls;
+  T* ychunk = yl + row0 * n * kC;
+  const uint32_t ebytes = (uint32_t)(rows_here * n * kC * sizeof(T));
+  const bool bulk_s = aligned16(src) && sbytes % 16 == 0;
+  const bool ycontig = a.contig && aligned16(ychunk) && ebytes % 16 == 0;
+  const bool bulk_e = UPDATE && ycontig;
+  if (threadIdx.x == 0) {
+    fail_flag = 0;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
   __syncthreads();
-  C* Z = fft_tile<+1>(A, B, tw, a.plan, W);
+  if (threadIdx.x == 0 && (bulk_s || bulk_e)) {
+    mbar_arrive_expect_tx(&bar, (bulk_s ? sbytes : 0u) + (bulk_e ? ebytes : 0u));
+    if (bulk_s) bulk_load(B, src, sbytes, &bar);
+    if (bulk_e) bulk_load(Eo, ychunk, ebytes, &bar);
+  }
+  if (!bulk_s) {
+    const int cnt = rows_here * m * kC;
+    for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) B[idx] = src[idx];
+  }
+  if (UPDATE && !bulk_e) {
+    for (int rr = 0; rr < rows_here; ++rr)
+      for (int e = threadIdx.x; e < n; e += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < kC; ++c)
+          Eo[(rr * n + e) * kC + c] = yl[geom_off(a.g, row0 + rr, e, c)];
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  if (bulk_s || bulk_e) {
+    if (!tile_wait(&bar, &fail_flag)) return;
+  } else {
+    __syncthreads();
+  }
+  const Lane ln = make_lane(W);
+  {
+    const int col = ln.col;
+    const int ra = 2 * col, rb = 2 * col + 1;
+    const int rra = ra / kC, ca = ra - rra * kC;
+    const int rrb = rb / kC, cb = rb - rrb * kC;
+    const bool va = ra < RC && rra < rows_here, vb = rb < RC && rrb < rows_here;
+    for (int k = ln.j0; k < n; k += ln.T) {
+      const bool mirror = 2 * k > n;
+      const int kk = mirror ? n - k : k;
+      C Av = mkc(T(0), T(0)), Bv = mkc(T(0), T(0));
+      if (va) Av = B[((int64_t)rra * m + kk) * kC + ca];
+      if (vb) Bv = B[((int64_t)rrb * m + kk) * kC + cb];
+      if (kk == 0 || 2 * kk == n) {
+        Av.y = T(0);
+        Bv.y = T(0);
+      }
+      A[k * W + col] = mirror ? mkc(Av.x + Bv.y, Bv.x - Av.y) : mkc(Av.x - Bv.y, Av.y + Bv.x);
+    }
+  }
+  __syncthreads();
+  C* Z = fft_tile<+1>(A, B, tw, a.plan, W, ln);
   const T* Zr = reinterpret_cast<const T*>(Z);
+  T* O = UPDATE ? Eo : reinterpret_cast<T*>(Z == A ? B : A);  // output staging [rr][e][c]
   double acc = 0.0;
-  T* yl = UPDATE ? nullptr : a.y + l * a.g.ls;
-  T* el = UPDATE ? reinterpret_cast<T*>(a.y) + l * a.g.ls : nullptr;
-  const int total = RC * n;
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int c = idx % Cc;
-    const int t = idx / Cc;
-    const int e = t % n;
-    const int rr = t / n;
-    if (rr < rows_here) {
-      const T v = Zr[e * ldr + rr * Cc + c];
-      const int64_t off = geom_off(a.g, row0 + rr, e, c);
-      if (UPDATE) {
-        const T old = el[off];
-        const T nv = sub_rn(static_cast<T>(a.E[l * Cc + c]), mul_rn(a.scale, v));
-        el[off] = nv;
-        const double d = static_cast<double>(nv) - static_cast<double>(old);
-        acc += d * d;
-      } else {
-        yl[off] = mul_rn(a.scale, v);
+  for (int rr = 0; rr < rows_here; ++rr)
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        const T v = Zr[e * ldr + rr * kC + c];
+        const int s = (rr * n + e) * kC + c;
+        if (UPDATE) {
+          const T old = O[s];
+          const T nv = sub_rn(static_cast<T>(a.E[l * kC + c]), mul_rn(a.scale, v));
+          O[s] = nv;
+          const double d = static_cast<double>(nv) - static_cast<double>(old);
+          acc += d * d;
+        } else {
+          O[s] = mul_rn(a.scale, v);
+        }
       }
     }
+  fence_async_shared();
+  __syncthreads();
+  if (ycontig) {
+    if (threadIdx.x == 0) {
+      bulk_store(ychunk, O, ebytes);
+      bulk_commit();
+      bulk_wait_read();
+    }
+  } else {
+    for (int rr = 0; rr < rows_here; ++rr)
+      for (int e = threadIdx.x; e < n; e += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < kC; ++c)
+          yl[geom_off(a.g, row0 + rr, e, c)] = O[(rr * n + e) * kC + c];
   }
   if (UPDATE) {
     const double s = block_sum(acc, red);
@@ -245,42 +359,77 @@ template <typename T> struct ColsArgs {
   GreenTables<T> gt;
 };
 
+// complex transform along a strided axis of [outer][n][inner]: a tile of n
+// rows x W consecutive columns, loaded and stored by one bulk copy per row
+// (issued by warp 0).  MODE 0/1: forward/inverse; MODE 2: forward, Green
+// contraction of each spectral coefficient (axis 0 index = tile row), inverse.
 template <typename T, int MODE, int DIM>
 __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
   using C = cx<T>;
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int fail_flag;
   const int n = a.plan.n, W = a.W;
   C* tw = reinterpret_cast<C*>(smem);
-  C* A = tw + n;
-  C* B = A + (size_t)n * W;
+  C* A = align16_ptr<C>(tw + n);
+  C* B = align16_ptr<C>(A + (size_t)n * W);
   const int64_t c0 = (int64_t)blockIdx.x * W;
   const int Wc = (int)min((int64_t)W, a.inner - c0);
   const int64_t o = blockIdx.y;
   const C* src = a.in + o * n * a.inner + c0;
   C* dst = a.out + o * n * a.inner + c0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
-  for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
-    const int e = idx / W;
-    const int col = idx - e * W;
-    A[idx] = col < Wc ? src[(int64_t)e * a.inner + col] : mkc(T(0), T(0));
+  const uint32_t rowbytes = (uint32_t)(Wc * sizeof(C));
+  const bool bulk = aligned16(src) && aligned16(dst) && ((a.inner * sizeof(C)) % 16 == 0) &&
+                    (rowbytes % 16 == 0) && ((W * sizeof(C)) % 16 == 0);
+  if (threadIdx.x == 0) {
+    fail_flag = 0;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
   __syncthreads();
+  if (bulk) {
+    if (threadIdx.x < 32) {
+      if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, rowbytes * (uint32_t)n);
+      __syncwarp();
+      for (int e = threadIdx.x; e < n; e += 32)
+        bulk_load(A + (size_t)e * W, src + (int64_t)e * a.inner, rowbytes, &bar);
+    }
+    if (Wc < W)
+      for (int idx = threadIdx.x; idx < n * (W - Wc); idx += blockDim.x) {
+        const int e = idx / (W - Wc);
+        A[e * W + Wc + (idx - e * (W - Wc))] = mkc(T(0), T(0));
+      }
+  } else {
+    for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
+      const int e = idx / W;
+      const int col = idx - e * W;
+      A[idx] = col < Wc ? src[(int64_t)e * a.inner + col] : mkc(T(0), T(0));
+    }
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  if (bulk) {
+    if (!tile_wait(&bar, &fail_flag)) return;
+  } else {
+    __syncthreads();
+  }
+  const Lane ln = make_lane(W);
   C* Z;
   if (MODE == 1)
-    Z = fft_tile<+1>(A, B, tw, a.plan, W);
+    Z = fft_tile<+1>(A, B, tw, a.plan, W, ln);
   else
-    Z = fft_tile<-1>(A, B, tw, a.plan, W);
+    Z = fft_tile<-1>(A, B, tw, a.plan, W, ln);
   if (MODE == 2) {
     const int Cc = a.C;
     const int Wf = W / Cc;
-    for (int idx = threadIdx.x; idx < n * Wf; idx += blockDim.x) {
-      const int e = idx / Wf;
-      const int fl = idx - e * Wf;
+    const int nthr = (blockDim.x / Wf) * Wf;
+    if ((int)threadIdx.x < nthr) {
+      const int fl = threadIdx.x % Wf;
+      const int e0 = threadIdx.x / Wf;
+      const int est = nthr / Wf;
       const int col0 = fl * Cc;
       if (col0 < Wc) {
         const int64_t f = (c0 + col0) / Cc;
         int b[3];
-        b[0] = e;
         if (DIM == 3) {
           b[1] = (int)(f / a.m_last);
           b[2] = (int)(f % a.m_last);
@@ -288,17 +437,31 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
           b[1] = (int)f;
           b[2] = 0;
         }
-        green_contract<DIM, T>(a.gt, b, Z + e * W + col0);
+        for (int e = e0; e < n; e += est) {
+          b[0] = e;
+          green_contract<DIM, T>(a.gt, b, Z + e * W + col0);
+        }
       }
     }
     __syncthreads();
     C* other = (Z == A) ? B : A;
-    Z = fft_tile<+1>(Z, other, tw, a.plan, W);
+    Z = fft_tile<+1>(Z, other, tw, a.plan, W, ln);
   }
-  for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
-    const int e = idx / W;
-    const int col = idx - e * W;
-    if (col < Wc) dst[(int64_t)e * a.inner + col] = Z[idx];
+  if (bulk) {
+    fence_async_shared();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      for (int e = threadIdx.x; e < n; e += 32)
+        bulk_store(dst + (int64_t)e * a.inner, Z + (size_t)e * W, rowbytes);
+      bulk_commit();
+      bulk_wait_read();
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
+      const int e = idx / W;
+      const int col = idx - e * W;
+      if (col < Wc) dst[(int64_t)e * a.inner + col] = Z[idx];
+    }
   }
 }
 
@@ -431,13 +594,24 @@ int grid_for(int64_t total) {
   return (int)g;
 }
 
-// rows per CTA and tile width for the contiguous-axis kernels
-bool rows_shape(int dtype, int n, int C, int* R, int* W, size_t* smem) {
+// threads per block for a W-column tile: the largest power-of-two number of
+// lanes per column T with T * W <= kThreads
+int tile_threads(int W) {
+  int t = 1;
+  while (2 * t * W <= kThreads) t *= 2;
+  return (t * W + 31) / 32 * 32;  // whole warps (block reductions use full-warp shuffles)
+}
+
+// rows per CTA, tile width and shared memory of the contiguous-axis kernels
+// (tiles of (n+2) x W complex, W = ceil(R*C/2); `extra` = the old-strain
+// staging of the update variant)
+bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem) {
   const size_t cs = dtype == F64 ? 16 : 8;
   int r = (24 + C - 1) / C;
   for (;;) {
     const int w = (r * C + 1) / 2;
-    const size_t bytes = n * cs + 2 * (size_t)(n + 2) * w * cs;
+    const size_t bytes = n * cs + 2 * (size_t)(n + 2) * w * cs +
+                         (update ? (size_t)r * n * C * (cs / 2) : 0) + 48;  // + alignment
     if (bytes <= kSmemBudget || r == 1) {
       if (bytes > kSmemCap - 4096) return false;
       *R = r;
@@ -451,10 +625,10 @@ bool rows_shape(int dtype, int n, int C, int* R, int* W, size_t* smem) {
 
 bool cols_shape(int dtype, int n, int unit, int* W, size_t* smem) {
   const size_t cs = dtype == F64 ? 16 : 8;
-  int w = unit * ((16 + unit / 2) / unit);
+  int w = unit == 1 ? 16 : unit * (12 / unit > 0 ? 12 / unit : 1);
   if (w < unit) w = unit;
   for (;;) {
-    const size_t bytes = n * cs + 2 * (size_t)n * w * cs;
+    const size_t bytes = n * cs + 2 * (size_t)n * w * cs + 32;  // + alignment
     if (bytes <= kSmemBudget || w == unit) {
       if (bytes > kSmemCap - 4096) return false;
       *W = w;
@@ -465,6 +639,30 @@ bool cols_shape(int dtype, int n, int unit, int* W, size_t* smem) {
   }
 }
 
+bool contiguous_rows(const RealGeom& g, int n, int C) {
+  if (g.cs != 1 || g.es != C) return false;
+  if (g.n1r == 1) return g.s0 == (int64_t)n * C;
+  return g.s1 == (int64_t)n * C && g.s0 == g.n1r * n * C;
+}
+
+template <typename T, int CC, bool LOCAL>
+cudaError_t r2c_go(const RowsArgs<T>& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(&rows_r2c_kernel<T, CC, LOCAL>);
+  cudaError_t e = ensure_smem(fn, smem);
+  if (e != cudaSuccess) return e;
+  rows_r2c_kernel<T, CC, LOCAL><<<grid, threads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int CC, bool UPDATE>
+cudaError_t c2r_go(const RowsArgs<T>& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, CC, UPDATE>);
+  cudaError_t e = ensure_smem(fn, smem);
+  if (e != cudaSuccess) return e;
+  rows_c2r_kernel<T, CC, UPDATE><<<grid, threads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const RealGeom& g,
                        void* out, const LocalDesc* local, cudaStream_t st) {
@@ -472,34 +670,33 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   int R, W;
   size_t smem;
   const int n = ax.plan.n;
-  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, &R, &W, &smem)) return cudaErrorInvalidValue;
+  if (C != 1 && C != 3 && C != 6) return cudaErrorInvalidValue;
+  if (local && C == 1) return cudaErrorInvalidValue;
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem))
+    return cudaErrorInvalidValue;
   a.x = static_cast<const T*>(x);
   a.out = static_cast<cx<T>*>(out);
   a.tw = static_cast<const cx<T>*>(ax.tw);
   a.plan = ax.plan;
   a.g = g;
-  a.C = C;
   a.R = R;
   a.W = W;
   a.m = n / 2 + 1;
+  a.contig = contiguous_rows(g, n, C);
   a.cstride_l = g.rows * a.m * C;
+  const int threads = tile_threads(W);
   dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
   if (local) {
     a.phase = local->phase;
     a.index_bytes = local->index_bytes;
     a.table = static_cast<const T*>(local->table);
     a.dim = local->dim;
-    const void* fn = reinterpret_cast<const void*>(&rows_r2c_kernel<T, true>);
-    cudaError_t e = ensure_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    rows_r2c_kernel<T, true><<<grid, kThreads, smem, st>>>(a);
-  } else {
-    const void* fn = reinterpret_cast<const void*>(&rows_r2c_kernel<T, false>);
-    cudaError_t e = ensure_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    rows_r2c_kernel<T, false><<<grid, kThreads, smem, st>>>(a);
+    return C == 3 ? r2c_go<T, 3, true>(a, grid, threads, smem, st)
+                  : r2c_go<T, 6, true>(a, grid, threads, smem, st);
   }
-  return cudaGetLastError();
+  if (C == 1) return r2c_go<T, 1, false>(a, grid, threads, smem, st);
+  if (C == 3) return r2c_go<T, 3, false>(a, grid, threads, smem, st);
+  return r2c_go<T, 6, false>(a, grid, threads, smem, st);
 }
 
 template <typename T>
@@ -510,34 +707,33 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
   int R, W;
   size_t smem;
   const int n = ax.plan.n;
-  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, &R, &W, &smem)) return cudaErrorInvalidValue;
+  if (C != 1 && C != 3 && C != 6) return cudaErrorInvalidValue;
+  if (upd && C == 1) return cudaErrorInvalidValue;
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, upd != nullptr, &R, &W, &smem))
+    return cudaErrorInvalidValue;
   a.cin = static_cast<const cx<T>*>(in);
   a.y = static_cast<T*>(upd ? upd->eps : y);
   a.tw = static_cast<const cx<T>*>(ax.tw);
   a.plan = ax.plan;
   a.g = g;
-  a.C = C;
   a.R = R;
   a.W = W;
   a.m = n / 2 + 1;
+  a.contig = contiguous_rows(g, n, C);
   a.cstride_l = g.rows * a.m * C;
   a.scale = static_cast<T>(scale);
+  const int threads = tile_threads(W);
   dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
   if (nb_out) *nb_out = (int)grid.x;
   if (upd) {
     a.E = upd->E;
     a.partials = upd->partials;
-    const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, true>);
-    cudaError_t e = ensure_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    rows_c2r_kernel<T, true><<<grid, kThreads, smem, st>>>(a);
-  } else {
-    const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, false>);
-    cudaError_t e = ensure_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    rows_c2r_kernel<T, false><<<grid, kThreads, smem, st>>>(a);
+    return C == 3 ? c2r_go<T, 3, true>(a, grid, threads, smem, st)
+                  : c2r_go<T, 6, true>(a, grid, threads, smem, st);
   }
-  return cudaGetLastError();
+  if (C == 1) return c2r_go<T, 1, false>(a, grid, threads, smem, st);
+  if (C == 3) return c2r_go<T, 3, false>(a, grid, threads, smem, st);
+  return c2r_go<T, 6, false>(a, grid, threads, smem, st);
 }
 
 template <typename T> GreenTables<T> to_tables(const GreenDeviceTables* gt) {
@@ -557,11 +753,12 @@ template <typename T> GreenTables<T> to_tables(const GreenDeviceTables* gt) {
 }
 
 template <typename T, int MODE, int DIM>
-cudaError_t cols_launch(const ColsArgs<T>& a, dim3 grid, size_t smem, cudaStream_t st) {
+cudaError_t cols_launch(const ColsArgs<T>& a, dim3 grid, int threads, size_t smem,
+                        cudaStream_t st) {
   const void* fn = reinterpret_cast<const void*>(&cols_kernel<T, MODE, DIM>);
   cudaError_t e = ensure_smem(fn, smem);
   if (e != cudaSuccess) return e;
-  cols_kernel<T, MODE, DIM><<<grid, kThreads, smem, st>>>(a);
+  cols_kernel<T, MODE, DIM><<<grid, threads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -586,16 +783,24 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
   a.C = C;
   a.m_last = m_last;
   a.gt = to_tables<T>(gt);
+  const int threads = tile_threads(W);
   dim3 grid((unsigned)((inner + W - 1) / W), (unsigned)outer);
-  if (mode == 0) return cols_launch<T, 0, 2>(a, grid, smem, st);
-  if (mode == 1) return cols_launch<T, 1, 2>(a, grid, smem, st);
-  if (dim == 2) return cols_launch<T, 2, 2>(a, grid, smem, st);
-  return cols_launch<T, 2, 3>(a, grid, smem, st);
+  if (mode == 0) return cols_launch<T, 0, 2>(a, grid, threads, smem, st);
+  if (mode == 1) return cols_launch<T, 1, 2>(a, grid, threads, smem, st);
+  if (dim == 2) return cols_launch<T, 2, 2>(a, grid, threads, smem, st);
+  return cols_launch<T, 2, 3>(a, grid, threads, smem, st);
 }
 
 }  // namespace
 
 int max_axis_length(int dtype) { return dtype == F64 ? 4096 : 8192; }
+
+cudaError_t read_and_clear_fault(unsigned* out) {
+  unsigned zero = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_jb_fault, sizeof(unsigned));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(g_jb_fault, &zero, sizeof(unsigned));
+}
 
 cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const void* x,
                             const RealGeom& g, void* out, const LocalDesc* local,

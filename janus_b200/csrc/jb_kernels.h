@@ -55,6 +55,8 @@ struct UpdateDesc {
 };
 
 int max_axis_length(int dtype);
+// bit 0: a kernel gave up a bounded wait (see jb_async.cuh); cleared on read
+cudaError_t read_and_clear_fault(unsigned* out);
 
 // r2c along the contiguous axis: real x (geom) -> complex out [L][rows][m][C].
 cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const void* x,
