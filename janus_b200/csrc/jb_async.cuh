@@ -7,6 +7,7 @@
 // copies, and the caller returns without touching the tile.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -91,6 +92,27 @@ __device__ __forceinline__ void bulk_wait_read() {
 // async-proxy (bulk copy) accesses
 __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// tiled tensor copies (TMA) through a CUtensorMap kernel parameter; no
+// multicast.  The box's innermost coordinate x times the element size is a
+// multiple of 16 bytes at every call site.
+__device__ __forceinline__ void tma_load_3d(void* sdst, const CUtensorMap* map, int x, int y,
+                                            int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(sdst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z,
+                                             const void* ssrc) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
+      ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(ssrc))
+      : "memory");
 }
 
 __device__ __forceinline__ bool aligned16(const void* p) {

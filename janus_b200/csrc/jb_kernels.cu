@@ -12,6 +12,9 @@
 // Spectral layout in HBM: complex [L][n0][(n1)][m][s], m = n_last/2 + 1,
 // Mandel component fastest (so one spectral coefficient's s components are
 // one contiguous 48-byte (3D) / 24-byte (2D) group in FP64 complex).
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
 #include <mutex>
 #include <unordered_map>
 
@@ -91,6 +94,7 @@ template <typename T> struct RowsArgs {
   AxisPlan plan;
   RealGeom g;
   int R, W, m;
+  int L;       // load cases (persistent kernels)
   int contig;  // real side rows are contiguous [rows][n][C]
   int64_t cstride_l;
   const void* phase;
@@ -354,6 +358,7 @@ template <typename T> struct ColsArgs {
   const cx<T>* tw;
   AxisPlan plan;
   int64_t inner;
+  int64_t outer;
   int W, C;
   int64_t m_last;
   GreenTables<T> gt;
@@ -463,6 +468,121 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
       if (col < Wc) dst[(int64_t)e * a.inner + col] = Z[idx];
     }
   }
+}
+
+// ===========================================================================
+// Persistent, software-pipelined forms of the three pass kernels.
+//
+// A grid of (SM count x resident CTAs) walks the tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...  Each CTA keeps two input buffers: while it
+// computes tile i, the bulk load of tile i+1 is in flight into the other
+// buffer and the bulk store of tile i-1 drains, so HBM traffic overlaps the
+// shared-memory FFT.  Before a buffer is reloaded the storing thread(s) wait
+// until their earlier bulk stores have finished reading shared memory.
+// These kernels are used when every tile satisfies the bulk-copy alignment
+// rules (checked on the host); otherwise the one-tile-per-CTA kernels above
+// run.
+// ===========================================================================
+
+template <typename P> __device__ __forceinline__ P* align128_ptr(void* p) {
+  return reinterpret_cast<P*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
+
+// Column pass with tensor TMA: the tile (n rows x W complex columns of
+// [outer][n][inner]) is one 3D box of the tensor map (split into boxes of at
+// most 256 rows), loaded into one of two input buffers while the previous
+// tile is computed, and stored back as boxes from shared memory.  Columns
+// past `inner` in the last chunk are zero-filled by the load and skipped by
+// the store.  Persistent grid; thread 0 issues all copies.
+template <typename T, int MODE, int DIM>
+__global__ void __launch_bounds__(kThreads)
+    cols_tma_kernel(const __grid_constant__ CUtensorMap tin,
+                    const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
+  using C = cx<T>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int fail_flag;
+  const int n = a.plan.n, W = a.W;
+  const size_t tile = (size_t)n * W;
+  C* tw = reinterpret_cast<C*>(smem);
+  C* In[2];
+  In[0] = align128_ptr<C>(tw + n);
+  In[1] = align128_ptr<C>(In[0] + tile);
+  C* Wk = align128_ptr<C>(In[1] + tile);
+  const int64_t ntx = (a.inner + W - 1) / W;
+  const int64_t total = ntx * a.outer;
+  if (threadIdx.x == 0) {
+    fail_flag = 0;
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  __syncthreads();
+  auto issue_load = [&](int64_t t, C* dst, uint64_t* b) {
+    const int64_t o = t / ntx;
+    const int x = (int)(2 * (t - o * ntx) * W);
+    mbar_arrive_expect_tx(b, (uint32_t)(tile * sizeof(C)));
+    for (int yb = 0; yb < n; yb += nbox) tma_load_3d(dst + (size_t)yb * W, &tin, x, yb, (int)o, b);
+  };
+  int64_t t = blockIdx.x;
+  if (t < total && threadIdx.x == 0) issue_load(t, In[0], &bar[0]);
+  const Lane ln = make_lane(W);
+  for (int i = 0; t < total; ++i, t += gridDim.x) {
+    const int buf = i & 1;
+    const int64_t o = t / ntx;
+    const int64_t c0 = (t - o * ntx) * W;
+    const int Wc = (int)min((int64_t)W, a.inner - c0);
+    C* in = In[buf];
+    if (!mbar_wait(&bar[buf], (i >> 1) & 1)) atomicOr(&fail_flag, 1);
+    if (threadIdx.x == 0) bulk_wait_read();  // the previous tile's stores have read smem
+    __syncthreads();
+    if (fail_flag) return;
+    const int64_t tn = t + gridDim.x;
+    if (threadIdx.x == 0 && tn < total) issue_load(tn, In[buf ^ 1], &bar[buf ^ 1]);
+    C* Z;
+    if (MODE == 1)
+      Z = fft_tile<+1>(in, Wk, tw, a.plan, W, ln);
+    else
+      Z = fft_tile<-1>(in, Wk, tw, a.plan, W, ln);
+    if (MODE == 2) {
+      const int Cc = a.C;
+      const int Wf = W / Cc;
+      const int nthr = (blockDim.x / Wf) * Wf;
+      if ((int)threadIdx.x < nthr) {
+        const int fl = threadIdx.x % Wf;
+        const int e0 = threadIdx.x / Wf;
+        const int est = nthr / Wf;
+        const int col0 = fl * Cc;
+        if (col0 < Wc) {
+          const int64_t f = (c0 + col0) / Cc;
+          int b[3];
+          if (DIM == 3) {
+            b[1] = (int)(f / a.m_last);
+            b[2] = (int)(f % a.m_last);
+          } else {
+            b[1] = (int)f;
+            b[2] = 0;
+          }
+          for (int e = e0; e < n; e += est) {
+            b[0] = e;
+            green_contract<DIM, T>(a.gt, b, Z + e * W + col0);
+          }
+        }
+      }
+      __syncthreads();
+      C* other = (Z == in) ? Wk : in;
+      Z = fft_tile<+1>(Z, other, tw, a.plan, W, ln);
+    }
+    fence_async_shared();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int x = (int)(2 * c0);
+      for (int yb = 0; yb < n; yb += nbox) tma_store_3d(&tout, x, yb, (int)o, Z + (size_t)yb * W);
+      bulk_commit();
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait_read();
 }
 
 template <typename T>
@@ -645,6 +765,95 @@ bool contiguous_rows(const RealGeom& g, int n, int C) {
   return g.s1 == (int64_t)n * C && g.s0 == g.n1r * n * C;
 }
 
+constexpr size_t kPipeBudget = 113 * 1024;  // two persistent CTAs per SM
+
+int sm_count() {
+  static int count = 0;
+  if (count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        count <= 0)
+      count = 148;
+  }
+  return count;
+}
+
+template <typename K>
+int persistent_grid(K kernel, int threads, size_t smem, int64_t tiles) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int64_t g = (int64_t)per_sm * sm_count();
+  return (int)(tiles < g ? tiles : g);
+}
+
+// tile width and shared memory of the tensor-TMA column kernel: two input
+// tiles and one compute partner of n x W complex, 128-byte aligned
+bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem) {
+  const size_t cs = dtype == F64 ? 16 : 8;
+  // measured on B200 (128^3 x 6, FP64): W = 8 columns for plain passes,
+  // 12 (two 6-component coefficients) for the Green pass
+  int w = unit == 1 ? 8 : unit * (12 / unit > 0 ? 12 / unit : 1);
+  if (const char* env = getenv("JB_COLS_W")) {
+    const int v = atoi(env);
+    if (v >= unit && v % unit == 0 && v <= 128) w = v;
+  }
+  if (w < unit) w = unit;
+  for (;; w -= unit) {
+    const size_t bytes = n * cs + 3 * 128 + 3 * (size_t)n * w * cs;
+    if (bytes <= kPipeBudget || w <= unit) {
+      if (bytes > kSmemCap - 4096 || (w * cs) % 16 != 0) return false;
+      *W = w;
+      *smem = bytes;
+      return true;
+    }
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// 3D map of a complex [outer][n][inner] array seen as reals [outer][n][2 inner],
+// box = 2W reals x nbox rows x 1
+bool make_cols_map(CUtensorMap* m, const void* base, bool f64, int64_t inner, int n,
+                   int64_t outer, int W, int nbox) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t rs = f64 ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)(2 * inner), (cuuint64_t)n, (cuuint64_t)outer};
+  cuuint64_t strides[2] = {(cuuint64_t)(2 * inner) * rs, (cuuint64_t)(2 * inner) * rs * n};
+  cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)nbox, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = enc(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         3, const_cast<void*>(base), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 template <typename T, int CC, bool LOCAL>
 cudaError_t r2c_go(const RowsArgs<T>& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
   const void* fn = reinterpret_cast<const void*>(&rows_r2c_kernel<T, CC, LOCAL>);
@@ -684,13 +893,16 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   a.m = n / 2 + 1;
   a.contig = contiguous_rows(g, n, C);
   a.cstride_l = g.rows * a.m * C;
-  const int threads = tile_threads(W);
-  dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
+  a.L = L;
   if (local) {
     a.phase = local->phase;
     a.index_bytes = local->index_bytes;
     a.table = static_cast<const T*>(local->table);
     a.dim = local->dim;
+  }
+  const int threads = tile_threads(W);
+  dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
+  if (local) {
     return C == 3 ? r2c_go<T, 3, true>(a, grid, threads, smem, st)
                   : r2c_go<T, 6, true>(a, grid, threads, smem, st);
   }
@@ -722,12 +934,15 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
   a.contig = contiguous_rows(g, n, C);
   a.cstride_l = g.rows * a.m * C;
   a.scale = static_cast<T>(scale);
+  a.L = L;
+  if (upd) {
+    a.E = upd->E;
+    a.partials = upd->partials;
+  }
   const int threads = tile_threads(W);
   dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
   if (nb_out) *nb_out = (int)grid.x;
   if (upd) {
-    a.E = upd->E;
-    a.partials = upd->partials;
     return C == 3 ? c2r_go<T, 3, true>(a, grid, threads, smem, st)
                   : c2r_go<T, 6, true>(a, grid, threads, smem, st);
   }
@@ -762,6 +977,18 @@ cudaError_t cols_launch(const ColsArgs<T>& a, dim3 grid, int threads, size_t sme
   return cudaGetLastError();
 }
 
+template <typename T, int MODE, int DIM>
+cudaError_t cols_tma_launch(const CUtensorMap& tin, const CUtensorMap& tout,
+                            const ColsArgs<T>& a, int nbox, int threads, size_t smem,
+                            int64_t tiles, cudaStream_t st) {
+  auto k = &cols_tma_kernel<T, MODE, DIM>;
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  const int grid = persistent_grid(k, threads, smem, tiles);
+  k<<<grid, threads, smem, st>>>(tin, tout, a, nbox);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, const void* in,
                    void* out, int C, int dim, const GreenDeviceTables* gt, int64_t m_last,
@@ -783,6 +1010,30 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
   a.C = C;
   a.m_last = m_last;
   a.gt = to_tables<T>(gt);
+  a.outer = outer;
+  {
+    int Wp;
+    size_t sp;
+    const size_t cs = sizeof(cx<T>);
+    if (al16(in) && al16(out) && (inner * cs) % 16 == 0 &&
+        cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &Wp, &sp)) {
+      int nbox = n <= 256 ? n : 256;  // rows per box: largest divisor of n up to 256
+      while (n % nbox != 0) --nbox;
+      CUtensorMap tin, tout;
+      if (nbox >= 8 &&
+          make_cols_map(&tin, in, sizeof(T) == 8, inner, n, outer, Wp, nbox) &&
+          make_cols_map(&tout, out, sizeof(T) == 8, inner, n, outer, Wp, nbox)) {
+        ColsArgs<T> b = a;
+        b.W = Wp;
+        const int thr = tile_threads(Wp);
+        const int64_t tiles = (inner + Wp - 1) / Wp * outer;
+        if (mode == 0) return cols_tma_launch<T, 0, 2>(tin, tout, b, nbox, thr, sp, tiles, st);
+        if (mode == 1) return cols_tma_launch<T, 1, 2>(tin, tout, b, nbox, thr, sp, tiles, st);
+        if (dim == 2) return cols_tma_launch<T, 2, 2>(tin, tout, b, nbox, thr, sp, tiles, st);
+        return cols_tma_launch<T, 2, 3>(tin, tout, b, nbox, thr, sp, tiles, st);
+      }
+    }
+  }
   const int threads = tile_threads(W);
   dim3 grid((unsigned)((inner + W - 1) / W), (unsigned)outer);
   if (mode == 0) return cols_launch<T, 0, 2>(a, grid, threads, smem, st);
