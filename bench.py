@@ -370,11 +370,30 @@ def run_gpu(args, rank, world, dist):
         rr = solver.run(E, args.solve_max_iter, tol=args.tol, eps=eps2, init=True)
         b.record()
         torch.cuda.synchronize()
-        solve = {"tol": args.tol, "iterations": rr.iterations,
-                 "seconds": round(a.elapsed_time(b) / 1e3, 4),
-                 "final_residual_max": float(rr.residuals[-1].max()),
-                 "C_eff_diag": [float(v) for v in np.diag(
-                     rr.mean_stress(material.create(*REF_MEDIUM, 3), E))]}
+        mat0 = material.create(*REF_MEDIUM, 3)
+        c64 = rr.mean_stress(mat0, E)
+        solve = {"tol": args.tol, "fp64": {
+            "iterations": rr.iterations, "seconds": round(a.elapsed_time(b) / 1e3, 4),
+            "final_residual_max": float(rr.residuals[-1].max()),
+            "C_eff_diag": [float(v) for v in np.diag(c64)]}}
+        if args.dtype == "f64":
+            from janus_b200.solvers import MixedScheme
+            mixed = MixedScheme(green, loc, nload=6, inner=args.inner)
+            eps3 = torch.empty_like(eps2)
+            mixed.run(E, tol=1e-3, max_outer=2, eps=eps3)  # warm the FP32 kernels
+            torch.cuda.synchronize()
+            a.record()
+            rm = mixed.run(E, tol=args.tol, max_outer=args.solve_max_iter)
+            b.record()
+            torch.cuda.synchronize()
+            cm = rm.mean_stress(mat0, E)
+            solve["mixed"] = {
+                "inner": args.inner, "outer_iterations": rm.outer_iterations,
+                "fp32_iterations": rm.fp32_iterations,
+                "seconds": round(a.elapsed_time(b) / 1e3, 4),
+                "final_residual_max": float(rm.residuals[-1].max()),
+                "C_eff_max_rel_diff_vs_fp64": float(np.abs(cm - c64).max() / np.abs(c64).max())}
+            solve["mixed_speedup"] = round(solve["fp64"]["seconds"] / solve["mixed"]["seconds"], 3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -443,6 +462,7 @@ def main(argv=None):
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--solve-max-iter", type=int, default=3000)
+    ap.add_argument("--inner", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-solve", action="store_true")

@@ -186,6 +186,29 @@ int jb_solver_set_load(jb_solver *solver, const double *E);
  * double[nload], may be NULL). */
 int jb_solver_step(jb_solver *solver, void *eps, double *res_dev,
                    void *stream);
+/* ---- mixed-precision basic scheme (defect correction) ------------------- */
+
+/* No counterpart in the reference (its solver loop is FP64 only).  Solves the
+ * same equation as jb_solver_run with FP32 bulk iterations and FP64 defect
+ * correction: each outer step computes, in FP64, the basic scheme's residual
+ * r = E - eps - Gamma0[(C - C0):eps] and its norm (the stopping test, same
+ * normalisation as jb_solver_run), then runs `inner - 1` FP32 iterations of
+ * d <- r - Gamma0[(C - C0):d] from d = r, and adds d to the FP64 eps.
+ * g64/l64 and g32/l32 are the same operators built with JB_F64 and JB_F32.
+ * The handles are borrowed and must outlive the solver. */
+typedef struct jb_mixed_s jb_mixed;
+int jb_mixed_create(jb_green *g64, jb_local *l64, jb_green *g32, jb_local *l32,
+                    int nload, jb_mixed **out);
+int jb_mixed_destroy(jb_mixed *solver);
+/* eps: device double[nload][grid][s]; E host double[nload][s]; residuals:
+ * host double[max_outer][nload] (FP64 residual at each outer step, may be
+ * NULL); outer_out / fp32_iters_out: counts done.  Returns after the work on
+ * `stream` has completed. */
+int jb_mixed_run(jb_mixed *solver, const double *E, void *eps, int init,
+                 int max_outer, int inner, double tol, double *residuals,
+                 int *outer_out, int *fp32_iters_out, double *mean_tau,
+                 void *stream);
+
 /* Benchmark support: record CUDA events around every pass of the next
  * `max_steps` calls of jb_solver_step (on their stream). */
 int jb_solver_timing_begin(jb_solver *solver, int max_steps);

@@ -69,6 +69,11 @@ _SIGS = {
     "jb_solver_timing_begin": ([c_void_p, c_int], c_int),
     "jb_solver_timing_end": ([c_void_p, P_double, P_int, P_int], c_int),
     "jb_solver_pass_name": ([c_void_p, c_int], ctypes.c_char_p),
+    "jb_mixed_create": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                         ctypes.POINTER(c_void_p)], c_int),
+    "jb_mixed_destroy": ([c_void_p], c_int),
+    "jb_mixed_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_int, c_double, P_double,
+                      P_int, P_int, P_double, c_void_p], c_int),
 }
 
 

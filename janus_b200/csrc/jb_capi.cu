@@ -1151,3 +1151,157 @@ extern "C" int jb_green_apply_noalloc(int dim, const int64_t* shape, double h, d
   for (int d = 0; d < 3; ++d) G.ax[d].tw = nullptr;  // not owned
   return r;
 }
+
+// ===========================================================================
+// mixed-precision basic scheme: FP32 bulk iterations, FP64 defect correction
+// ===========================================================================
+
+struct jb_mixed_s {
+  jb_green* g64 = nullptr;
+  jb_local* l64 = nullptr;
+  jb_green* g32 = nullptr;
+  jb_local* l32 = nullptr;
+  int L = 1;
+  DeviceBuf spec, partials, E, res, normd, r32, d32, mean;
+  std::vector<double> norm;
+};
+
+extern "C" int jb_mixed_create(jb_green* g64, jb_local* l64, jb_green* g32, jb_local* l32,
+                               int nload, jb_mixed** out) {
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  if (!g64 || !l64 || !g32 || !l32) return fail(JB_EINVAL, "NULL argument");
+  if (g64->dtype != F64 || l64->dtype != F64 || g32->dtype != F32 || l32->dtype != F32)
+    return fail(JB_EINVAL, "jb_mixed_create needs FP64 and FP32 operator pairs");
+  if (nload < 1 || nload > 65535) return fail(JB_EINVAL, "nload must be in [1, 65535]");
+  const int dim = g64->dim;
+  if (g32->dim != dim || l64->dim != dim || l32->dim != dim)
+    return fail(JB_EINVAL, "operators differ in dim");
+  for (int d = 0; d < dim; ++d)
+    if (g32->n[d] != g64->n[d] || l64->n[d] != g64->n[d] || l32->n[d] != g64->n[d])
+      return fail(JB_EINVAL, "operators differ in shape");
+  if (g32->variant != g64->variant || g32->g != g64->g || g32->nu != g64->nu ||
+      g32->h != g64->h)
+    return fail(JB_EINVAL, "FP32 and FP64 Green operators differ");
+  jb_mixed* M = new jb_mixed();
+  M->g64 = g64;
+  M->l64 = l64;
+  M->g32 = g32;
+  M->l32 = l32;
+  M->L = nload;
+  const int C = dim == 2 ? 3 : 6;
+  const int64_t nvox = l64->nvox;
+  const int64_t rows = dim == 2 ? g64->n[0] : g64->n[0] * g64->n[1];
+  int r = ensure_buf(M->spec, (size_t)nload * spec_elems(g64) * 16);
+  if (r == JB_OK) r = ensure_buf(M->partials, sizeof(double) * nload *
+                                                  std::max<int64_t>(rows, 1024 * C));
+  if (r == JB_OK) r = ensure_buf(M->E, sizeof(double) * nload * C);
+  if (r == JB_OK) r = ensure_buf(M->res, sizeof(double) * nload);
+  if (r == JB_OK) r = ensure_buf(M->normd, sizeof(double) * nload);
+  if (r == JB_OK) r = ensure_buf(M->mean, sizeof(double) * nload * C);
+  if (r == JB_OK) r = ensure_buf(M->r32, sizeof(float) * nload * nvox * C);
+  if (r == JB_OK) r = ensure_buf(M->d32, sizeof(float) * nload * nvox * C);
+  if (r != JB_OK) {
+    jb_mixed_destroy(M);
+    return r;
+  }
+  *out = M;
+  return JB_OK;
+}
+
+extern "C" int jb_mixed_destroy(jb_mixed* M) {
+  if (!M) return JB_OK;
+  for (DeviceBuf* b : {&M->spec, &M->partials, &M->E, &M->res, &M->normd, &M->r32, &M->d32,
+                       &M->mean})
+    if (b->p) cudaFree(b->p);
+  delete M;
+  return JB_OK;
+}
+
+extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, int max_outer,
+                            int inner, double tol, double* residuals, int* outer_out,
+                            int* fp32_iters_out, double* mean_tau, void* stream) {
+  if (!M || !E || !eps) return fail(JB_EINVAL, "NULL argument");
+  if (max_outer < 0) return fail(JB_EINVAL, "max_outer must be >= 0");
+  if (inner < 1) return fail(JB_EINVAL, "inner must be >= 1");
+  cudaStream_t st = as_stream(stream);
+  const int dim = M->g64->dim;
+  const int C = dim == 2 ? 3 : 6;
+  const int L = M->L;
+  const int64_t nvox = M->l64->nvox;
+  const int64_t nel = (int64_t)L * nvox * C;
+  double N = 1;
+  for (int d = 0; d < dim; ++d) N *= (double)M->g64->n[d];
+  M->norm.resize(L);
+  for (int l = 0; l < L; ++l) {
+    double s = 0;
+    for (int c = 0; c < C; ++c) s += E[l * C + c] * E[l * C + c];
+    if (!(s > 0)) return fail(JB_EINVAL, "macroscopic strain must be nonzero");
+    M->norm[l] = 1.0 / std::sqrt(N) / std::sqrt(s);
+  }
+  JB_CUDA(cudaMemcpyAsync(M->E.p, E, sizeof(double) * L * C, cudaMemcpyHostToDevice, st));
+  JB_CUDA(cudaMemcpyAsync(M->normd.p, M->norm.data(), sizeof(double) * L,
+                          cudaMemcpyHostToDevice, st));
+  if (init)
+    JB_TRY(launch_status(jb::launch_fill_macro(F64, C, L, nvox,
+                                               static_cast<const double*>(M->E.p), eps, st),
+                         "fill"));
+  jb::LocalDesc loc64 = local_desc(M->l64), loc32 = local_desc(M->l32);
+  float* r32 = static_cast<float*>(M->r32.p);
+  float* d32 = static_cast<float*>(M->d32.p);
+  std::vector<double> r(L);
+  int outer = 0, fp32 = 0;
+  for (; outer < max_outer; ++outer) {
+    jb::UpdateDesc u;
+    u.mode = 2;
+    u.eps = eps;
+    u.E = static_cast<const double*>(M->E.p);
+    u.partials = static_cast<double*>(M->partials.p);
+    u.rout = r32;
+    int nb = 0;
+    JB_TRY(green_passes(M->g64, eps, eps, L, M->spec.p, &loc64, &u, &nb, st));
+    JB_TRY(launch_status(jb::launch_reduce_rows(static_cast<const double*>(M->partials.p), L,
+                                                nb, static_cast<double*>(M->res.p), 1.0,
+                                                static_cast<const double*>(M->normd.p), 1, st),
+                         "reduce"));
+    JB_CUDA(cudaMemcpyAsync(r.data(), M->res.p, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
+    JB_CUDA(cudaStreamSynchronize(st));
+    bool done = true;
+    for (int l = 0; l < L; ++l) {
+      if (residuals) residuals[(size_t)outer * L + l] = r[l];
+      if (!(r[l] <= tol)) done = false;
+    }
+    if (done) {
+      ++outer;
+      break;
+    }
+    // correction: d = r, then inner - 1 FP32 sweeps of d <- r - Gamma0[(C-C0):d]
+    JB_CUDA(cudaMemcpyAsync(d32, r32, sizeof(float) * nel, cudaMemcpyDeviceToDevice, st));
+    for (int j = 1; j < inner; ++j) {
+      jb::UpdateDesc v;
+      v.mode = 3;
+      v.eps = d32;
+      v.rhs = r32;
+      JB_TRY(green_passes(M->g32, d32, d32, L, M->spec.p, &loc32, &v, nullptr, st));
+      ++fp32;
+    }
+    JB_TRY(launch_status(jb::launch_axpy_f32_to_f64(nel, d32, static_cast<double*>(eps), st),
+                         "axpy"));
+  }
+  if (outer_out) *outer_out = outer;
+  if (fp32_iters_out) *fp32_iters_out = fp32;
+  if (mean_tau) {
+    int nb = 0;
+    JB_TRY(launch_status(jb::launch_local_sum(F64, loc64, C, L, nvox, eps,
+                                              static_cast<double*>(M->partials.p), &nb, st),
+                         "local_sum"));
+    JB_TRY(launch_status(jb::launch_reduce_cols(static_cast<const double*>(M->partials.p), L, C,
+                                                nb, static_cast<double*>(M->mean.p),
+                                                1.0 / (double)nvox, st),
+                         "reduce"));
+    JB_CUDA(cudaMemcpyAsync(mean_tau, M->mean.p, sizeof(double) * L * C, cudaMemcpyDeviceToHost,
+                            st));
+  }
+  JB_CUDA(cudaStreamSynchronize(st));
+  return JB_OK;
+}

@@ -14,6 +14,8 @@
 // one contiguous 48-byte (3D) / 24-byte (2D) group in FP64 complex).
 #include <cudaTypedefs.h>
 
+#include <type_traits>
+
 #include <cstdlib>
 #include <mutex>
 #include <unordered_map>
@@ -103,6 +105,8 @@ template <typename T> struct RowsArgs {
   int dim;
   const double* E;
   double* partials;
+  const T* rhs;   // kEpiRhs: right-hand side field
+  float* rout;    // kEpiResid: FP32 residual field
   T scale;
 };
 
@@ -232,22 +236,30 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
 }
 
 // c2r along the contiguous axis; the spectral chunk (and, for the solver
-// update, the old strain chunk) arrive by bulk copies; the output chunk
-// leaves by one bulk copy.  UPDATE: eps <- E - scale * y in place with FP64
-// residual partials (sum of squared increments) per block.
-template <typename T, int CC, bool UPDATE>
+// epilogues, one real side field) arrive by bulk copies; the output chunk
+// leaves by one bulk copy.  Epilogues (y = scale * c2r(spectrum)):
+//   kEpiPlain : out = y
+//   kEpiUpdate: eps <- E - y in place, partials += (new - old)^2
+//   kEpiResid : r = (E - y) - eps written as FP32 to `rout` (eps unchanged),
+//               partials += r^2 (the basic scheme's increment, FP64)
+//   kEpiRhs   : d <- rhs - y in place (rhs a field of the same type)
+enum { kEpiPlain = 0, kEpiUpdate = 1, kEpiResid = 2, kEpiRhs = 3 };
+
+template <typename T, int CC, int EPI>
 __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   using C = cx<T>;
+  using OT = typename std::conditional<EPI == kEpiResid, float, T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int fail_flag;
   __shared__ double red[kThreads / 32];
   constexpr int kC = CC;
+  constexpr bool kSide = EPI != kEpiPlain;
   const int n = a.plan.n, W = a.W, R = a.R, m = a.m;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
   C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
-  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W);  // [R][n][CC] (UPDATE)
+  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W);  // [R][n][CC] side-field staging
   const int ldr = 2 * W;
   const int l = blockIdx.y;
   const int64_t row0 = (int64_t)blockIdx.x * R;
@@ -255,12 +267,17 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   const int RC = R * kC;
   const C* src = a.cin + l * a.cstride_l + row0 * m * kC;
   const uint32_t sbytes = (uint32_t)(rows_here * m * kC * sizeof(C));
-  T* yl = a.y + l * a.g.ls;
-  T* ychunk = yl + row0 * n * kC;
+  // side field: old eps (update, resid) or the right-hand side (rhs)
+  const T* sidel = (EPI == kEpiRhs ? a.rhs : a.y) + l * a.g.ls;
+  const T* sidechunk = sidel + row0 * n * kC;
+  OT* outl = (EPI == kEpiResid ? reinterpret_cast<OT*>(a.rout) : reinterpret_cast<OT*>(a.y)) +
+             l * a.g.ls;
+  OT* outchunk = outl + row0 * n * kC;
   const uint32_t ebytes = (uint32_t)(rows_here * n * kC * sizeof(T));
+  const uint32_t obytes = (uint32_t)(rows_here * n * kC * sizeof(OT));
   const bool bulk_s = aligned16(src) && sbytes % 16 == 0;
-  const bool ycontig = a.contig && aligned16(ychunk) && ebytes % 16 == 0;
-  const bool bulk_e = UPDATE && ycontig;
+  const bool bulk_e = kSide && a.contig && aligned16(sidechunk) && ebytes % 16 == 0;
+  const bool bulk_o = a.contig && aligned16(outchunk) && obytes % 16 == 0;
   if (threadIdx.x == 0) {
     fail_flag = 0;
     mbar_init(&bar, 1);
@@ -270,18 +287,18 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   if (threadIdx.x == 0 && (bulk_s || bulk_e)) {
     mbar_arrive_expect_tx(&bar, (bulk_s ? sbytes : 0u) + (bulk_e ? ebytes : 0u));
     if (bulk_s) bulk_load(B, src, sbytes, &bar);
-    if (bulk_e) bulk_load(Eo, ychunk, ebytes, &bar);
+    if (bulk_e) bulk_load(Eo, sidechunk, ebytes, &bar);
   }
   if (!bulk_s) {
     const int cnt = rows_here * m * kC;
     for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) B[idx] = src[idx];
   }
-  if (UPDATE && !bulk_e) {
+  if (kSide && !bulk_e) {
     for (int rr = 0; rr < rows_here; ++rr)
       for (int e = threadIdx.x; e < n; e += blockDim.x)
 #pragma unroll
         for (int c = 0; c < kC; ++c)
-          Eo[(rr * n + e) * kC + c] = yl[geom_off(a.g, row0 + rr, e, c)];
+          Eo[(rr * n + e) * kC + c] = sidel[geom_off(a.g, row0 + rr, e, c)];
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
   if (bulk_s || bulk_e) {
@@ -312,7 +329,9 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   __syncthreads();
   C* Z = fft_tile<+1>(A, B, tw, a.plan, W, ln);
   const T* Zr = reinterpret_cast<const T*>(Z);
-  T* O = UPDATE ? Eo : reinterpret_cast<T*>(Z == A ? B : A);  // output staging [rr][e][c]
+  // output staging [rr][e][c]: in place over the side field, or the free tile
+  OT* O = (EPI == kEpiUpdate || EPI == kEpiRhs) ? reinterpret_cast<OT*>(Eo)
+                                                : reinterpret_cast<OT*>(Z == A ? B : A);
   double acc = 0.0;
   for (int rr = 0; rr < rows_here; ++rr)
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
@@ -320,22 +339,29 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
       for (int c = 0; c < kC; ++c) {
         const T v = Zr[e * ldr + rr * kC + c];
         const int s = (rr * n + e) * kC + c;
-        if (UPDATE) {
-          const T old = O[s];
+        if (EPI == kEpiUpdate) {
+          const T old = Eo[s];
           const T nv = sub_rn(static_cast<T>(a.E[l * kC + c]), mul_rn(a.scale, v));
           O[s] = nv;
           const double d = static_cast<double>(nv) - static_cast<double>(old);
           acc += d * d;
+        } else if (EPI == kEpiResid) {
+          const T nv = sub_rn(static_cast<T>(a.E[l * kC + c]), mul_rn(a.scale, v));
+          const double d = static_cast<double>(nv) - static_cast<double>(Eo[s]);
+          O[s] = static_cast<OT>(d);
+          acc += d * d;
+        } else if (EPI == kEpiRhs) {
+          O[s] = static_cast<OT>(sub_rn(Eo[s], mul_rn(a.scale, v)));
         } else {
-          O[s] = mul_rn(a.scale, v);
+          O[s] = static_cast<OT>(mul_rn(a.scale, v));
         }
       }
     }
   fence_async_shared();
   __syncthreads();
-  if (ycontig) {
+  if (bulk_o) {
     if (threadIdx.x == 0) {
-      bulk_store(ychunk, O, ebytes);
+      bulk_store(outchunk, O, obytes);
       bulk_commit();
       bulk_wait_read();
     }
@@ -344,9 +370,9 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
       for (int e = threadIdx.x; e < n; e += blockDim.x)
 #pragma unroll
         for (int c = 0; c < kC; ++c)
-          yl[geom_off(a.g, row0 + rr, e, c)] = O[(rr * n + e) * kC + c];
+          outl[geom_off(a.g, row0 + rr, e, c)] = O[(rr * n + e) * kC + c];
   }
-  if (UPDATE) {
+  if (EPI == kEpiUpdate || EPI == kEpiResid) {
     const double s = block_sum(acc, red);
     if (threadIdx.x == 0) a.partials[(int64_t)l * gridDim.x + blockIdx.x] = s;
   }
@@ -658,6 +684,34 @@ __global__ void green_by_freq_kernel(GreenTables<T> gt, int64_t count, const int
   }
 }
 
+__global__ void axpy_f32_to_f64_kernel(int64_t n, const float* __restrict__ d,
+                                       double* __restrict__ y) {
+  const int64_t n4 = n / 4;
+  const float4* d4 = reinterpret_cast<const float4*>(d);
+  double2* y2 = reinterpret_cast<double2*>(y);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float4 v = d4[i];
+    double2 a = y2[2 * i], b = y2[2 * i + 1];
+    a.x += v.x;
+    a.y += v.y;
+    b.x += v.z;
+    b.y += v.w;
+    y2[2 * i] = a;
+    y2[2 * i + 1] = b;
+  }
+  for (int64_t i = 4 * n4 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += d[i];
+}
+
+__global__ void convert_f64_to_f32_kernel(int64_t n, const double* __restrict__ x,
+                                          float* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = static_cast<float>(x[i]);
+}
+
 template <typename T>
 __global__ void fill_macro_kernel(int C, int L, int64_t nvox, const double* E, T* eps) {
   const int64_t total = (int64_t)L * nvox * C;
@@ -863,13 +917,21 @@ cudaError_t r2c_go(const RowsArgs<T>& a, dim3 grid, int threads, size_t smem, cu
   return cudaGetLastError();
 }
 
-template <typename T, int CC, bool UPDATE>
+template <typename T, int CC, int EPI>
 cudaError_t c2r_go(const RowsArgs<T>& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
-  const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, CC, UPDATE>);
+  const void* fn = reinterpret_cast<const void*>(&rows_c2r_kernel<T, CC, EPI>);
   cudaError_t e = ensure_smem(fn, smem);
   if (e != cudaSuccess) return e;
-  rows_c2r_kernel<T, CC, UPDATE><<<grid, threads, smem, st>>>(a);
+  rows_c2r_kernel<T, CC, EPI><<<grid, threads, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+template <typename T, int EPI>
+cudaError_t c2r_go_c(int C, const RowsArgs<T>& a, dim3 grid, int threads, size_t smem,
+                     cudaStream_t st) {
+  if (C == 3) return c2r_go<T, 3, EPI>(a, grid, threads, smem, st);
+  if (C == 6) return c2r_go<T, 6, EPI>(a, grid, threads, smem, st);
+  return cudaErrorInvalidValue;
 }
 
 template <typename T>
@@ -935,20 +997,30 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
   a.cstride_l = g.rows * a.m * C;
   a.scale = static_cast<T>(scale);
   a.L = L;
+  const int epi = upd ? upd->mode : kEpiPlain;
   if (upd) {
     a.E = upd->E;
     a.partials = upd->partials;
+    a.rhs = static_cast<const T*>(upd->rhs);
+    a.rout = upd->rout;
+    if ((epi == kEpiResid || epi == kEpiRhs) && !a.contig) return cudaErrorInvalidValue;
+    if (epi == kEpiResid && (sizeof(T) != 8 || !upd->rout)) return cudaErrorInvalidValue;
+    if (epi == kEpiRhs && !upd->rhs) return cudaErrorInvalidValue;
   }
   const int threads = tile_threads(W);
   dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
   if (nb_out) *nb_out = (int)grid.x;
-  if (upd) {
-    return C == 3 ? c2r_go<T, 3, true>(a, grid, threads, smem, st)
-                  : c2r_go<T, 6, true>(a, grid, threads, smem, st);
+  switch (epi) {
+    case kEpiUpdate: return c2r_go_c<T, kEpiUpdate>(C, a, grid, threads, smem, st);
+    case kEpiResid:
+      if constexpr (sizeof(T) == 8) return c2r_go_c<T, kEpiResid>(C, a, grid, threads, smem, st);
+      return cudaErrorInvalidValue;
+    case kEpiRhs: return c2r_go_c<T, kEpiRhs>(C, a, grid, threads, smem, st);
+    default: break;
   }
-  if (C == 1) return c2r_go<T, 1, false>(a, grid, threads, smem, st);
-  if (C == 3) return c2r_go<T, 3, false>(a, grid, threads, smem, st);
-  return c2r_go<T, 6, false>(a, grid, threads, smem, st);
+  if (C == 1) return c2r_go<T, 1, kEpiPlain>(a, grid, threads, smem, st);
+  if (C == 3) return c2r_go<T, 3, kEpiPlain>(a, grid, threads, smem, st);
+  return c2r_go<T, 6, kEpiPlain>(a, grid, threads, smem, st);
 }
 
 template <typename T> GreenTables<T> to_tables(const GreenDeviceTables* gt) {
@@ -1152,6 +1224,19 @@ cudaError_t launch_fill_macro(int dtype, int C, int L, int64_t nvox, const doubl
     fill_macro_kernel<double><<<grid, kThreads, 0, st>>>(C, L, nvox, E, static_cast<double*>(eps));
   else
     fill_macro_kernel<float><<<grid, kThreads, 0, st>>>(C, L, nvox, E, static_cast<float*>(eps));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStream_t st) {
+  const bool vec = (reinterpret_cast<uintptr_t>(d) & 15u) == 0 &&
+                   (reinterpret_cast<uintptr_t>(y) & 15u) == 0;
+  if (!vec) return cudaErrorInvalidValue;
+  axpy_f32_to_f64_kernel<<<grid_for(n / 4 + 1), kThreads, 0, st>>>(n, d, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_f64_to_f32(int64_t n, const double* x, float* y, cudaStream_t st) {
+  convert_f64_to_f32_kernel<<<grid_for(n), kThreads, 0, st>>>(n, x, y);
   return cudaGetLastError();
 }
 

@@ -47,12 +47,23 @@ struct LocalDesc {
   int dim = 2;
 };
 
-// Solver update of the last pass: eps = E - scale * y, residual partials.
+// Solver epilogue of the last pass (y = scale * c2r(spectrum)):
+//  mode 1: eps <- E - y in place, partials = sum (new - old)^2
+//  mode 2: rout <- (E - y) - eps as FP32 (FP64 fields only), partials = sum r^2
+//  mode 3: eps <- rhs - y in place (rhs a field of the same type)
 struct UpdateDesc {
-  void* eps = nullptr;          // field updated in place (layout of RealGeom)
+  int mode = 1;
+  void* eps = nullptr;          // field read/updated (layout of RealGeom)
   const double* E = nullptr;    // device [L][C] macroscopic strains (FP64)
   double* partials = nullptr;   // device [L][gridDim.x]
+  const void* rhs = nullptr;    // mode 3
+  float* rout = nullptr;        // mode 2
 };
+
+// y[i] += (double) d[i] over n elements (FP64 field, FP32 correction)
+cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStream_t st);
+// y[i] = (float) x[i]
+cudaError_t launch_convert_f64_to_f32(int64_t n, const double* x, float* y, cudaStream_t st);
 
 int max_axis_length(int dtype);
 // bit 0: a kernel gave up a bounded wait (see jb_async.cuh); cleared on read

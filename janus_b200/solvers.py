@@ -149,3 +149,88 @@ def basic_scheme(green_op, local_op, avg_eps, num_iter, tol=0.0, eps=None):
     """Run the basic scheme for one or several load cases (rows of avg_eps)."""
     E = np.atleast_2d(np.asarray(avg_eps, dtype=np.float64))
     return BasicScheme(green_op, local_op, E.shape[0]).run(E, num_iter, tol, eps)
+
+
+@dataclass
+class MixedResult:
+    eps: torch.Tensor          # (nload,) + grid + (s,), FP64 on the device
+    residuals: np.ndarray      # (outer steps, nload): FP64 residual at each outer step
+    outer_iterations: int
+    fp32_iterations: int
+    mean_tau: np.ndarray       # (nload, s)
+
+    def mean_stress(self, mat0, avg_eps):
+        return _c0_apply(mat0, np.atleast_2d(avg_eps)) + self.mean_tau
+
+
+class MixedScheme:
+    """Mixed-precision basic scheme: FP32 bulk iterations with FP64 defect
+    correction (no counterpart in the reference, whose loop is FP64).
+
+    Every outer step evaluates the FP64 residual r = E - eps - Gamma0[(C -
+    C0):eps] (whose normalised norm is the stopping test, as for
+    BasicScheme), runs ``inner - 1`` FP32 iterations d <- r - Gamma0[(C -
+    C0):d] from d = r, and adds d to the FP64 strain field.  The FP32
+    operators are built from the given FP64 ones (same material, grid,
+    discretisation and phase map)."""
+
+    def __init__(self, green_op, local_op, nload=1, inner=20):
+        if isinstance(local_op, _BlockDiagonalOperator):
+            local = local_op.local
+        else:
+            local = local_op
+        if not isinstance(local, LocalPhaseOperator):
+            raise ValueError("the solver needs isotropic local operators (phase map)")
+        if green_op.dtype != torch.float64 or local.dtype != torch.float64:
+            raise ValueError("MixedScheme takes the FP64 operators")
+        self.green_op = green_op
+        self.local = local
+        self.nload = int(nload)
+        self.inner = int(inner)
+        self.green32 = type(green_op)(green_op.green, green_op.ishape[:-1], green_op.h,
+                                      dtype=torch.float32)
+        self.local32 = LocalPhaseOperator(local.dim, local.shape, local.phase, local.sph,
+                                          local.dev, dtype=torch.float32)
+        self._handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().jb_mixed_create(green_op.handle, local.handle, self.green32.handle,
+                                              self.local32.handle, self.nload,
+                                              ctypes.byref(self._handle)))
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().jb_mixed_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    @property
+    def field_shape(self):
+        return (self.nload,) + tuple(self.green_op.ishape)
+
+    def run(self, avg_eps, tol, max_outer=1000, eps=None, inner=None):
+        E = np.ascontiguousarray(np.asarray(avg_eps, dtype=np.float64).reshape(
+            self.nload, self.green_op.ishape[-1]))
+        init = eps is None
+        if eps is None:
+            eps = torch.empty(self.field_shape, dtype=torch.float64, device=A.device())
+        elif tuple(eps.shape) != self.field_shape or eps.dtype != torch.float64 or \
+                not eps.is_contiguous() or eps.device.type != "cuda":
+            raise ValueError("eps must be a contiguous FP64 CUDA tensor of shape {0}".format(
+                self.field_shape))
+        inner = self.inner if inner is None else int(inner)
+        res = np.zeros((max(int(max_outer), 1), self.nload))
+        outer = ctypes.c_int(0)
+        fp32 = ctypes.c_int(0)
+        mean = np.zeros((self.nload, self.green_op.ishape[-1]))
+        P = ctypes.POINTER(ctypes.c_double)
+        _lib.check(_lib.lib().jb_mixed_run(self._handle, E.ctypes.data_as(P),
+                                           ctypes.c_void_p(eps.data_ptr()),
+                                           int(init), int(max_outer), inner, float(tol),
+                                           res.ctypes.data_as(P), ctypes.byref(outer),
+                                           ctypes.byref(fp32), mean.ctypes.data_as(P),
+                                           ctypes.c_void_p(A.stream_handle())))
+        n = outer.value
+        return MixedResult(eps=eps, residuals=res[:n].copy(), outer_iterations=n,
+                           fp32_iterations=fp32.value, mean_tau=mean)
