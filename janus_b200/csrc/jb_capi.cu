@@ -800,6 +800,7 @@ static jb::LocalDesc local_desc(const jb_local* L) {
   d.phase = L->phase;
   d.index_bytes = L->index_bytes;
   d.table = L->table;
+  d.nphase = L->nphase;
   d.dim = L->dim;
   return d;
 }

@@ -105,6 +105,153 @@ __device__ __forceinline__ void gamma2_acc(T k0, T k1, T w, const C* t, C* acc, 
   }
 }
 
+// Filtered operator as accumulated tensors.  With q_a = 1/|k_a|^2,
+// alpha_a = w_a q_a / (2g) and beta_a = alpha_a q_a / (1 - nu),
+//   sum_a w_a Gamma(k_a):t = M t + t M - N:t,
+//   M = sum_a alpha_a k_a (x) k_a,  N = sum_a beta_a k_a (x) k_a (x) k_a (x) k_a,
+// so the 2^d aliases cost one symmetric rank-2 and one fully symmetric
+// rank-4 accumulation each, and the contraction is done once per part.
+// FP64 computes the 2^d reciprocals with one division (batched inversion:
+// prefix products, one reciprocal, back substitution).
+template <typename T, int NA>
+__device__ __forceinline__ void batch_reciprocal(T* x) {
+  if constexpr (sizeof(T) == 8) {
+    T pre[NA];
+    pre[0] = x[0];
+#pragma unroll
+    for (int i = 1; i < NA; ++i) pre[i] = pre[i - 1] * x[i];
+    T inv = T(1) / pre[NA - 1];
+#pragma unroll
+    for (int i = NA - 1; i > 0; --i) {
+      const T xi = x[i];
+      x[i] = inv * pre[i - 1];
+      inv *= xi;
+    }
+    x[0] = inv;
+  } else {
+#pragma unroll
+    for (int i = 0; i < NA; ++i) x[i] = T(1) / x[i];
+  }
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ void green_filtered3(const GreenTables<T>& g, const int* b, C* te) {
+  const T kx[2] = {g.kn[0][b[0]], g.kp[0][b[0]]}, wx[2] = {g.wn[0][b[0]], g.wp[0][b[0]]};
+  const T ky[2] = {g.kn[1][b[1]], g.kp[1][b[1]]}, wy[2] = {g.wn[1][b[1]], g.wp[1][b[1]]};
+  const T kz[2] = {g.kn[2][b[2]], g.kp[2][b[2]]}, wz[2] = {g.wn[2][b[2]], g.wp[2][b[2]]};
+  T q[8];
+  bool zero[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const T k0 = kx[a >> 2], k1 = ky[(a >> 1) & 1], k2 = kz[a & 1];
+    const T kk = k0 * k0 + k1 * k1 + k2 * k2;
+    zero[a] = kk == T(0);
+    q[a] = zero[a] ? T(1) : kk;
+  }
+  batch_reciprocal<T, 8>(q);
+  // M: m00 m11 m22 m12 m20 m01; N: fully symmetric quartic moments
+  T m00 = 0, m11 = 0, m22 = 0, m12 = 0, m20 = 0, m01 = 0;
+  T n400 = 0, n040 = 0, n004 = 0, n220 = 0, n202 = 0, n022 = 0, n310 = 0, n301 = 0, n130 = 0,
+    n031 = 0, n103 = 0, n013 = 0, n211 = 0, n121 = 0, n112 = 0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    if (zero[a]) continue;
+    const T k0 = kx[a >> 2], k1 = ky[(a >> 1) & 1], k2 = kz[a & 1];
+    const T w = wx[a >> 2] * wy[(a >> 1) & 1] * wz[a & 1];
+    const T al = w * q[a] * g.inv2g;
+    const T be = al * q[a] * g.c1;
+    const T p00 = k0 * k0, p11 = k1 * k1, p22 = k2 * k2;
+    const T p12 = k1 * k2, p20 = k2 * k0, p01 = k0 * k1;
+    m00 += al * p00; m11 += al * p11; m22 += al * p22;
+    m12 += al * p12; m20 += al * p20; m01 += al * p01;
+    const T b00 = be * p00, b11 = be * p11, b22 = be * p22;
+    n400 += b00 * p00; n040 += b11 * p11; n004 += b22 * p22;
+    n220 += b00 * p11; n202 += b00 * p22; n022 += b11 * p22;
+    n310 += b00 * p01; n301 += b00 * p20; n130 += b11 * p01;
+    n031 += b11 * p12; n103 += b22 * p20; n013 += b22 * p12;
+    n211 += b00 * p12; n121 += b11 * p20; n112 += b22 * p01;
+  }
+  const T u = T(0.70710678118654752440084436210485);
+  const T s2 = T(1.4142135623730950488016887242097);
+#pragma unroll
+  for (int part = 0; part < 2; ++part) {
+    const T t00 = part ? te[0].y : te[0].x;
+    const T t11 = part ? te[1].y : te[1].x;
+    const T t22 = part ? te[2].y : te[2].x;
+    const T t12 = u * (part ? te[3].y : te[3].x);
+    const T t20 = u * (part ? te[4].y : te[4].x);
+    const T t01 = u * (part ? te[5].y : te[5].x);
+    const T S00 = n400 * t00 + n220 * t11 + n202 * t22 + T(2) * (n211 * t12 + n301 * t20 + n310 * t01);
+    const T S11 = n220 * t00 + n040 * t11 + n022 * t22 + T(2) * (n031 * t12 + n121 * t20 + n130 * t01);
+    const T S22 = n202 * t00 + n022 * t11 + n004 * t22 + T(2) * (n013 * t12 + n103 * t20 + n112 * t01);
+    const T S12 = n211 * t00 + n031 * t11 + n013 * t22 + T(2) * (n022 * t12 + n112 * t20 + n121 * t01);
+    const T S20 = n301 * t00 + n121 * t11 + n103 * t22 + T(2) * (n112 * t12 + n202 * t20 + n211 * t01);
+    const T S01 = n310 * t00 + n130 * t11 + n112 * t22 + T(2) * (n121 * t12 + n211 * t20 + n220 * t01);
+    const T P00 = T(2) * (m00 * t00 + m01 * t01 + m20 * t20);
+    const T P11 = T(2) * (m01 * t01 + m11 * t11 + m12 * t12);
+    const T P22 = T(2) * (m20 * t20 + m12 * t12 + m22 * t22);
+    const T P12 = (m11 + m22) * t12 + m12 * (t11 + t22) + m01 * t20 + m20 * t01;
+    const T P20 = (m22 + m00) * t20 + m20 * (t22 + t00) + m12 * t01 + m01 * t12;
+    const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11) + m20 * t12 + m12 * t20;
+    const T o0 = P00 - S00, o1 = P11 - S11, o2 = P22 - S22;
+    const T o3 = s2 * (P12 - S12), o4 = s2 * (P20 - S20), o5 = s2 * (P01 - S01);
+    if (part == 0) {
+      te[0].x = o0; te[1].x = o1; te[2].x = o2; te[3].x = o3; te[4].x = o4; te[5].x = o5;
+    } else {
+      te[0].y = o0; te[1].y = o1; te[2].y = o2; te[3].y = o3; te[4].y = o4; te[5].y = o5;
+    }
+  }
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ void green_filtered2(const GreenTables<T>& g, const int* b, C* te) {
+  const T kx[2] = {g.kn[0][b[0]], g.kp[0][b[0]]}, wx[2] = {g.wn[0][b[0]], g.wp[0][b[0]]};
+  const T ky[2] = {g.kn[1][b[1]], g.kp[1][b[1]]}, wy[2] = {g.wn[1][b[1]], g.wp[1][b[1]]};
+  T q[4];
+  bool zero[4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const T k0 = kx[a >> 1], k1 = ky[a & 1];
+    const T kk = k0 * k0 + k1 * k1;
+    zero[a] = kk == T(0);
+    q[a] = zero[a] ? T(1) : kk;
+  }
+  batch_reciprocal<T, 4>(q);
+  T m00 = 0, m11 = 0, m01 = 0, n40 = 0, n31 = 0, n22 = 0, n13 = 0, n04 = 0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    if (zero[a]) continue;
+    const T k0 = kx[a >> 1], k1 = ky[a & 1];
+    const T w = wx[a >> 1] * wy[a & 1];
+    const T al = w * q[a] * g.inv2g;
+    const T be = al * q[a] * g.c1;
+    const T p00 = k0 * k0, p11 = k1 * k1, p01 = k0 * k1;
+    m00 += al * p00; m11 += al * p11; m01 += al * p01;
+    const T b00 = be * p00, b11 = be * p11;
+    n40 += b00 * p00; n31 += b00 * p01; n22 += b00 * p11; n13 += b11 * p01; n04 += b11 * p11;
+  }
+  const T u = T(0.70710678118654752440084436210485);
+  const T s2 = T(1.4142135623730950488016887242097);
+#pragma unroll
+  for (int part = 0; part < 2; ++part) {
+    const T t00 = part ? te[0].y : te[0].x;
+    const T t11 = part ? te[1].y : te[1].x;
+    const T t01 = u * (part ? te[2].y : te[2].x);
+    const T S00 = n40 * t00 + n22 * t11 + T(2) * n31 * t01;
+    const T S11 = n22 * t00 + n04 * t11 + T(2) * n13 * t01;
+    const T S01 = n31 * t00 + n13 * t11 + T(2) * n22 * t01;
+    const T P00 = T(2) * (m00 * t00 + m01 * t01);
+    const T P11 = T(2) * (m01 * t01 + m11 * t11);
+    const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11);
+    const T o0 = P00 - S00, o1 = P11 - S11, o2 = s2 * (P01 - S01);
+    if (part == 0) {
+      te[0].x = o0; te[1].x = o1; te[2].x = o2;
+    } else {
+      te[0].y = o0; te[1].y = o1; te[2].y = o2;
+    }
+  }
+}
+
 // eta = Gamma_discrete(b) : tau for one half-spectrum index b (b[d] < n_d).
 // tau and eta may alias.
 template <int DIM, typename T, typename C>
@@ -123,26 +270,12 @@ __device__ __forceinline__ void green_contract(const GreenTables<T>& g, const in
     else
       gamma3_acc(g.kt[0][b[0]], g.kt[1][b[1]], g.kt[2][b[2]], T(1), t, acc, g.inv2g, g.c1);
   } else {
-    if (DIM == 2) {
-      const T kn0 = g.kn[0][b[0]], kp0 = g.kp[0][b[0]], wn0 = g.wn[0][b[0]], wp0 = g.wp[0][b[0]];
-      const T kn1 = g.kn[1][b[1]], kp1 = g.kp[1][b[1]], wn1 = g.wn[1][b[1]], wp1 = g.wp[1][b[1]];
-      gamma2_acc(kn0, kn1, wn0 * wn1, t, acc, g.inv2g, g.c1);
-      gamma2_acc(kn0, kp1, wn0 * wp1, t, acc, g.inv2g, g.c1);
-      gamma2_acc(kp0, kn1, wp0 * wn1, t, acc, g.inv2g, g.c1);
-      gamma2_acc(kp0, kp1, wp0 * wp1, t, acc, g.inv2g, g.c1);
-    } else {
-      const T kn0 = g.kn[0][b[0]], kp0 = g.kp[0][b[0]], wn0 = g.wn[0][b[0]], wp0 = g.wp[0][b[0]];
-      const T kn1 = g.kn[1][b[1]], kp1 = g.kp[1][b[1]], wn1 = g.wn[1][b[1]], wp1 = g.wp[1][b[1]];
-      const T kn2 = g.kn[2][b[2]], kp2 = g.kp[2][b[2]], wn2 = g.wn[2][b[2]], wp2 = g.wp[2][b[2]];
-      gamma3_acc(kn0, kn1, kn2, wn0 * wn1 * wn2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kn0, kn1, kp2, wn0 * wn1 * wp2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kn0, kp1, kn2, wn0 * wp1 * wn2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kn0, kp1, kp2, wn0 * wp1 * wp2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kp0, kn1, kn2, wp0 * wn1 * wn2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kp0, kn1, kp2, wp0 * wn1 * wp2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kp0, kp1, kn2, wp0 * wp1 * wn2, t, acc, g.inv2g, g.c1);
-      gamma3_acc(kp0, kp1, kp2, wp0 * wp1 * wp2, t, acc, g.inv2g, g.c1);
-    }
+    if (DIM == 2)
+      green_filtered2<T>(g, b, t);
+    else
+      green_filtered3<T>(g, b, t);
+#pragma unroll
+    for (int i = 0; i < S; ++i) acc[i] = t[i];
   }
 #pragma unroll
   for (int i = 0; i < S; ++i) tau_eta[i] = acc[i];

@@ -31,6 +31,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr size_t kSmemCap = 227 * 1024;
 constexpr size_t kSmemBudget = 96 * 1024;
+constexpr int kTabStage = 512;  // phase tables up to this size are staged in smem
 
 template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
 template <> __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
@@ -102,6 +103,7 @@ template <typename T> struct RowsArgs {
   const void* phase;
   int index_bytes;
   const T* table;
+  int nphase;  // table entries (staged in shared memory when <= kTabStage)
   int dim;
   const double* E;
   double* partials;
@@ -176,6 +178,19 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
           Br[(rr * n + e) * kC + c] = xl[geom_off(a.g, row0 + rr, e, c)];
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  // local operator: phase ids of the tile and the (tr, dev) table go to
+  // shared memory while the bulk copy is in flight
+  int* phs = reinterpret_cast<int*>(B + (size_t)(n + 2) * W);
+  T* tabs = align16_ptr<T>(phs + (size_t)R * n);
+  const T* tab = a.table;
+  if constexpr (LOCAL) {
+    for (int i = threadIdx.x; i < rows_here * n; i += blockDim.x)
+      phs[i] = load_phase(a.phase, a.index_bytes, row0 * n + i);
+    if (a.nphase <= kTabStage) {
+      for (int i = threadIdx.x; i < 2 * a.nphase; i += blockDim.x) tabs[i] = a.table[i];
+      tab = tabs;
+    }
+  }
   if (bulk) {
     if (!tile_wait(&bar, &fail_flag)) return;
   } else {
@@ -188,8 +203,8 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
 #pragma unroll
         for (int c = 0; c < kC; ++c) v[c] = Br[(rr * n + e) * kC + c];
         if constexpr (LOCAL) {
-          const int ph = load_phase(a.phase, a.index_bytes, (row0 + rr) * n + e);
-          iso_apply<T>(v, a.table[2 * ph], a.table[2 * ph + 1], kC == 3 ? 2 : 3);
+          const int ph = phs[rr * n + e];
+          iso_apply<T>(v, tab[2 * ph], tab[2 * ph + 1], kC == 3 ? 2 : 3);
         }
       } else {
 #pragma unroll
@@ -333,6 +348,10 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   OT* O = (EPI == kEpiUpdate || EPI == kEpiRhs) ? reinterpret_cast<OT*>(Eo)
                                                 : reinterpret_cast<OT*>(Z == A ? B : A);
   double acc = 0.0;
+  T Ev[kC];
+#pragma unroll
+  for (int c = 0; c < kC; ++c)
+    Ev[c] = (EPI == kEpiUpdate || EPI == kEpiResid) ? static_cast<T>(a.E[l * kC + c]) : T(0);
   for (int rr = 0; rr < rows_here; ++rr)
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
 #pragma unroll
@@ -341,12 +360,12 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
         const int s = (rr * n + e) * kC + c;
         if (EPI == kEpiUpdate) {
           const T old = Eo[s];
-          const T nv = sub_rn(static_cast<T>(a.E[l * kC + c]), mul_rn(a.scale, v));
+          const T nv = sub_rn(Ev[c], mul_rn(a.scale, v));
           O[s] = nv;
           const double d = static_cast<double>(nv) - static_cast<double>(old);
           acc += d * d;
         } else if (EPI == kEpiResid) {
-          const T nv = sub_rn(static_cast<T>(a.E[l * kC + c]), mul_rn(a.scale, v));
+          const T nv = sub_rn(Ev[c], mul_rn(a.scale, v));
           const double d = static_cast<double>(nv) - static_cast<double>(Eo[s]);
           O[s] = static_cast<OT>(d);
           acc += d * d;
@@ -779,13 +798,16 @@ int tile_threads(int W) {
 // rows per CTA, tile width and shared memory of the contiguous-axis kernels
 // (tiles of (n+2) x W complex, W = ceil(R*C/2); `extra` = the old-strain
 // staging of the update variant)
-bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem) {
+bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem,
+                bool local = false) {
   const size_t cs = dtype == F64 ? 16 : 8;
   int r = (24 + C - 1) / C;
   for (;;) {
     const int w = (r * C + 1) / 2;
     const size_t bytes = n * cs + 2 * (size_t)(n + 2) * w * cs +
-                         (update ? (size_t)r * n * C * (cs / 2) : 0) + 48;  // + alignment
+                         (update ? (size_t)r * n * C * (cs / 2) : 0) +
+                         (local ? (size_t)r * n * 4 + 2 * kTabStage * (cs / 2) + 16 : 0) +
+                         48;  // + alignment
     if (bytes <= kSmemBudget || r == 1) {
       if (bytes > kSmemCap - 4096) return false;
       *R = r;
@@ -943,7 +965,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   const int n = ax.plan.n;
   if (C != 1 && C != 3 && C != 6) return cudaErrorInvalidValue;
   if (local && C == 1) return cudaErrorInvalidValue;
-  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem))
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem, local != nullptr))
     return cudaErrorInvalidValue;
   a.x = static_cast<const T*>(x);
   a.out = static_cast<cx<T>*>(out);
@@ -960,6 +982,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     a.phase = local->phase;
     a.index_bytes = local->index_bytes;
     a.table = static_cast<const T*>(local->table);
+    a.nphase = local->nphase;
     a.dim = local->dim;
   }
   const int threads = tile_threads(W);

@@ -44,6 +44,7 @@ struct LocalDesc {
   const void* phase = nullptr;  // uint8 or int32 per voxel, row-major grid
   int index_bytes = 1;          // 1 or 4
   const void* table = nullptr;  // device, T[2 * nphase]
+  int nphase = 1;
   int dim = 2;
 };
 
