@@ -133,6 +133,42 @@ template <int DIR, typename C> struct Dft<8, DIR, C> {
   }
 };
 
+template <int DIR, typename C> struct Dft<16, DIR, C> {
+  // 16 = 4 x 4: DFT4 over stride-4 groups, twiddles w16^(j q), DFT4 across
+  __device__ __forceinline__ static void run(C* v) {
+    using T = decltype(v[0].x);
+    const T c1 = T(0.92387953251128675612818318939679);  // cos(pi/8)
+    const T s1 = T(0.38268343236508977172845998403040);  // sin(pi/8)
+    const T h = T(0.70710678118654752440084436210485);
+    C a[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      C g[4] = {v[j], v[j + 4], v[j + 8], v[j + 12]};
+      Dft<4, DIR, C>::run(g);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) a[j][q] = g[q];
+    }
+    // w16^(DIR m) = cos(m pi/8) + DIR i sin(m pi/8), m = j q
+    auto rot = [&](C x, T c, T s) { return mkc(x.x * c - DIR * x.y * s, x.y * c + DIR * x.x * s); };
+    a[1][1] = rot(a[1][1], c1, s1);
+    a[1][2] = rot(a[1][2], h, h);
+    a[1][3] = rot(a[1][3], s1, c1);
+    a[2][1] = rot(a[2][1], h, h);
+    a[2][2] = mul_i<DIR>(a[2][2]);
+    a[2][3] = rot(a[2][3], -h, h);
+    a[3][1] = rot(a[3][1], s1, c1);
+    a[3][2] = rot(a[3][2], -h, h);
+    a[3][3] = rot(a[3][3], -c1, -s1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      C g[4] = {a[0][q], a[1][q], a[2][q], a[3][q]};
+      Dft<4, DIR, C>::run(g);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) v[q + 4 * p] = g[p];
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // one Stockham stage over a W-column tile
 // ---------------------------------------------------------------------------

@@ -21,6 +21,7 @@
 #include <unordered_map>
 
 #include "jb_async.cuh"
+#include "jb_fft_ct.cuh"
 #include "jb_green.cuh"
 #include "jb_kernels.h"
 
@@ -137,13 +138,16 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* fail_flag) {
 //  3. Stockham FFT of the W complex columns (real columns paired as re/im);
 //  4. split into the two half spectra, staged as [rr][k][c] and written out
 //     by one bulk copy.
-template <typename T, int CC, bool LOCAL>
+template <typename T, int CC, bool LOCAL, int NCT = 0, int WCT = 0>
 __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int fail_flag;
-  const int n = a.plan.n, W = a.W, R = a.R, m = a.m;
+  const int n = NCT > 0 ? NCT : a.plan.n;
+  const int W = WCT > 0 ? WCT : a.W;
+  const int R = WCT > 0 ? 2 * WCT / CC : a.R;
+  const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
   C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
@@ -218,7 +222,11 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
       for (int j = RC; j < ldr; ++j) Ar[e * ldr + j] = T(0);
   __syncthreads();
   const Lane ln = make_lane(W);
-  C* Z = fft_tile<-1>(A, B, tw, a.plan, W, ln);
+  C* Z;
+  if constexpr (NCT > 0)
+    Z = fft_ct<NCT, WCT, -1>(A, B, tw);
+  else
+    Z = fft_tile<-1>(A, B, tw, a.plan, W, ln);
   C* S = (Z == A) ? B : A;
   {
     const int col = ln.col;
@@ -260,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
 //   kEpiRhs   : d <- rhs - y in place (rhs a field of the same type)
 enum { kEpiPlain = 0, kEpiUpdate = 1, kEpiResid = 2, kEpiRhs = 3 };
 
-template <typename T, int CC, int EPI>
+template <typename T, int CC, int EPI, int NCT = 0, int WCT = 0>
 __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   using OT = typename std::conditional<EPI == kEpiResid, float, T>::type;
@@ -270,7 +278,10 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   __shared__ double red[kThreads / 32];
   constexpr int kC = CC;
   constexpr bool kSide = EPI != kEpiPlain;
-  const int n = a.plan.n, W = a.W, R = a.R, m = a.m;
+  const int n = NCT > 0 ? NCT : a.plan.n;
+  const int W = WCT > 0 ? WCT : a.W;
+  const int R = WCT > 0 ? 2 * WCT / CC : a.R;
+  const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
   C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
@@ -342,7 +353,11 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
     }
   }
   __syncthreads();
-  C* Z = fft_tile<+1>(A, B, tw, a.plan, W, ln);
+  C* Z;
+  if constexpr (NCT > 0)
+    Z = fft_ct<NCT, WCT, +1>(A, B, tw);
+  else
+    Z = fft_tile<+1>(A, B, tw, a.plan, W, ln);
   const T* Zr = reinterpret_cast<const T*>(Z);
   // output staging [rr][e][c]: in place over the side field, or the free tile
   OT* O = (EPI == kEpiUpdate || EPI == kEpiRhs) ? reinterpret_cast<OT*>(Eo)
@@ -539,7 +554,7 @@ template <typename P> __device__ __forceinline__ P* align128_ptr(void* p) {
 // tile is computed, and stored back as boxes from shared memory.  Columns
 // past `inner` in the last chunk are zero-filled by the load and skipped by
 // the store.  Persistent grid; thread 0 issues all copies.
-template <typename T, int MODE, int DIM>
+template <typename T, int MODE, int DIM, int NCT = 0, int WCT = 0>
 __global__ void __launch_bounds__(kThreads)
     cols_tma_kernel(const __grid_constant__ CUtensorMap tin,
                     const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
@@ -547,7 +562,8 @@ __global__ void __launch_bounds__(kThreads)
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int fail_flag;
-  const int n = a.plan.n, W = a.W;
+  const int n = NCT > 0 ? NCT : a.plan.n;
+  const int W = WCT > 0 ? WCT : a.W;
   const size_t tile = (size_t)n * W;
   C* tw = reinterpret_cast<C*>(smem);
   C* In[2];
@@ -586,10 +602,17 @@ __global__ void __launch_bounds__(kThreads)
     const int64_t tn = t + gridDim.x;
     if (threadIdx.x == 0 && tn < total) issue_load(tn, In[buf ^ 1], &bar[buf ^ 1]);
     C* Z;
-    if (MODE == 1)
-      Z = fft_tile<+1>(in, Wk, tw, a.plan, W, ln);
-    else
-      Z = fft_tile<-1>(in, Wk, tw, a.plan, W, ln);
+    if constexpr (NCT > 0) {
+      if (MODE == 1)
+        Z = fft_ct<NCT, WCT, +1>(in, Wk, tw);
+      else
+        Z = fft_ct<NCT, WCT, -1>(in, Wk, tw);
+    } else {
+      if (MODE == 1)
+        Z = fft_tile<+1>(in, Wk, tw, a.plan, W, ln);
+      else
+        Z = fft_tile<-1>(in, Wk, tw, a.plan, W, ln);
+    }
     if (MODE == 2) {
       const int Cc = a.C;
       const int Wf = W / Cc;
@@ -617,7 +640,10 @@ __global__ void __launch_bounds__(kThreads)
       }
       __syncthreads();
       C* other = (Z == in) ? Wk : in;
-      Z = fft_tile<+1>(Z, other, tw, a.plan, W, ln);
+      if constexpr (NCT > 0)
+        Z = fft_ct<NCT, WCT, +1>(Z, other, tw);
+      else
+        Z = fft_tile<+1>(Z, other, tw, a.plan, W, ln);
     }
     fence_async_shared();
     __syncthreads();
@@ -798,6 +824,12 @@ int tile_threads(int W) {
 // rows per CTA, tile width and shared memory of the contiguous-axis kernels
 // (tiles of (n+2) x W complex, W = ceil(R*C/2); `extra` = the old-strain
 // staging of the update variant)
+size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local) {
+  const size_t cs = dtype == F64 ? 16 : 8;
+  return n * cs + 2 * (size_t)(n + 2) * w * cs + (update ? (size_t)r * n * C * (cs / 2) : 0) +
+         (local ? (size_t)r * n * 4 + 2 * kTabStage * (cs / 2) + 16 : 0) + 48;
+}
+
 bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem,
                 bool local = false) {
   const size_t cs = dtype == F64 ? 16 : 8;
@@ -956,6 +988,50 @@ cudaError_t c2r_go_c(int C, const RowsArgs<T>& a, dim3 grid, int threads, size_t
   return cudaErrorInvalidValue;
 }
 
+template <typename T, int CC, bool LOCAL, int N, int W>
+cudaError_t r2c_ct_go(const RowsArgs<T>& a, dim3 grid, size_t smem, cudaStream_t st) {
+  auto k = &rows_r2c_kernel<T, CC, LOCAL, N, W>;
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, ct_threads<N, W>(), smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int CC, int EPI, int N, int W>
+cudaError_t c2r_ct_go(const RowsArgs<T>& a, dim3 grid, size_t smem, cudaStream_t st) {
+  auto k = &rows_c2r_kernel<T, CC, EPI, N, W>;
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, ct_threads<N, W>(), smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// cudaErrorNotSupported: no compile-time variant for this combination
+template <typename T, int N, int W>
+cudaError_t c2r_ct_dispatch(int C, int epi, const RowsArgs<T>& a, dim3 grid, size_t smem,
+                            cudaStream_t st) {
+  if (C == 6) {
+    switch (epi) {
+      case kEpiPlain: return c2r_ct_go<T, 6, kEpiPlain, N, W>(a, grid, smem, st);
+      case kEpiUpdate: return c2r_ct_go<T, 6, kEpiUpdate, N, W>(a, grid, smem, st);
+      case kEpiResid:
+        if constexpr (sizeof(T) == 8) return c2r_ct_go<T, 6, kEpiResid, N, W>(a, grid, smem, st);
+        return cudaErrorInvalidValue;
+      case kEpiRhs: return c2r_ct_go<T, 6, kEpiRhs, N, W>(a, grid, smem, st);
+    }
+  } else if (C == 3) {
+    switch (epi) {
+      case kEpiPlain: return c2r_ct_go<T, 3, kEpiPlain, N, W>(a, grid, smem, st);
+      case kEpiUpdate: return c2r_ct_go<T, 3, kEpiUpdate, N, W>(a, grid, smem, st);
+      case kEpiResid:
+        if constexpr (sizeof(T) == 8) return c2r_ct_go<T, 3, kEpiResid, N, W>(a, grid, smem, st);
+        return cudaErrorInvalidValue;
+      case kEpiRhs: return c2r_ct_go<T, 3, kEpiRhs, N, W>(a, grid, smem, st);
+    }
+  }
+  return cudaErrorNotSupported;
+}
+
 template <typename T>
 cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const RealGeom& g,
                        void* out, const LocalDesc* local, cudaStream_t st) {
@@ -984,6 +1060,34 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     a.table = static_cast<const T*>(local->table);
     a.nphase = local->nphase;
     a.dim = local->dim;
+  }
+  if ((n == 64 || n == 128 || n == 256) && (C == 3 || C == 6)) {
+    // compile-time tiles: W = 12 columns (6 for n = 256), R = 2 W / C rows
+    const int wct = n <= 128 ? 12 : 6;
+    const int rct = 2 * wct / C;
+    const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, false,
+                                 local != nullptr);
+    if (sct <= kSmemBudget + 24 * 1024) {
+      RowsArgs<T> b = a;
+      b.R = rct;
+      b.W = wct;
+      dim3 grid((unsigned)((g.rows + rct - 1) / rct), (unsigned)L);
+      switch (n * 16 + C * 2 + (local ? 1 : 0)) {
+        case 64 * 16 + 6: return r2c_ct_go<T, 3, false, 64, 12>(b, grid, sct, st);
+        case 64 * 16 + 7: return r2c_ct_go<T, 3, true, 64, 12>(b, grid, sct, st);
+        case 64 * 16 + 12: return r2c_ct_go<T, 6, false, 64, 12>(b, grid, sct, st);
+        case 64 * 16 + 13: return r2c_ct_go<T, 6, true, 64, 12>(b, grid, sct, st);
+        case 128 * 16 + 6: return r2c_ct_go<T, 3, false, 128, 12>(b, grid, sct, st);
+        case 128 * 16 + 7: return r2c_ct_go<T, 3, true, 128, 12>(b, grid, sct, st);
+        case 128 * 16 + 12: return r2c_ct_go<T, 6, false, 128, 12>(b, grid, sct, st);
+        case 128 * 16 + 13: return r2c_ct_go<T, 6, true, 128, 12>(b, grid, sct, st);
+        case 256 * 16 + 6: return r2c_ct_go<T, 3, false, 256, 6>(b, grid, sct, st);
+        case 256 * 16 + 7: return r2c_ct_go<T, 3, true, 256, 6>(b, grid, sct, st);
+        case 256 * 16 + 12: return r2c_ct_go<T, 6, false, 256, 6>(b, grid, sct, st);
+        case 256 * 16 + 13: return r2c_ct_go<T, 6, true, 256, 6>(b, grid, sct, st);
+        default: break;
+      }
+    }
   }
   const int threads = tile_threads(W);
   dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
@@ -1030,6 +1134,24 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
     if (epi == kEpiResid && (sizeof(T) != 8 || !upd->rout)) return cudaErrorInvalidValue;
     if (epi == kEpiRhs && !upd->rhs) return cudaErrorInvalidValue;
   }
+  if ((n == 64 || n == 128 || n == 256) && (C == 3 || C == 6)) {
+    const int wct = n <= 128 ? 12 : 6;
+    const int rct = 2 * wct / C;
+    const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, upd != nullptr,
+                                 false);
+    if (sct <= kSmemBudget + 24 * 1024) {
+      RowsArgs<T> b = a;
+      b.R = rct;
+      b.W = wct;
+      dim3 grid((unsigned)((g.rows + rct - 1) / rct), (unsigned)L);
+      if (nb_out) *nb_out = (int)grid.x;
+      cudaError_t e = cudaErrorNotSupported;
+      if (n == 64) e = c2r_ct_dispatch<T, 64, 12>(C, epi, b, grid, sct, st);
+      if (n == 128) e = c2r_ct_dispatch<T, 128, 12>(C, epi, b, grid, sct, st);
+      if (n == 256) e = c2r_ct_dispatch<T, 256, 6>(C, epi, b, grid, sct, st);
+      if (e != cudaErrorNotSupported) return e;
+    }
+  }
   const int threads = tile_threads(W);
   dim3 grid((unsigned)((g.rows + R - 1) / R), (unsigned)L);
   if (nb_out) *nb_out = (int)grid.x;
@@ -1070,6 +1192,29 @@ cudaError_t cols_launch(const ColsArgs<T>& a, dim3 grid, int threads, size_t sme
   if (e != cudaSuccess) return e;
   cols_kernel<T, MODE, DIM><<<grid, threads, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+template <typename T, int MODE, int DIM, int N, int W>
+cudaError_t cols_ct_launch(const CUtensorMap& tin, const CUtensorMap& tout,
+                           const ColsArgs<T>& a, int nbox, size_t smem, int64_t tiles,
+                           cudaStream_t st) {
+  auto k = &cols_tma_kernel<T, MODE, DIM, N, W>;
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  const int threads = ct_threads<N, W>();
+  const int grid = persistent_grid(k, threads, smem, tiles);
+  k<<<grid, threads, smem, st>>>(tin, tout, a, nbox);
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t cols_ct_dispatch(int mode, int dim, const CUtensorMap& tin, const CUtensorMap& tout,
+                             const ColsArgs<T>& a, int nbox, size_t smem, int64_t tiles,
+                             cudaStream_t st) {
+  if (mode == 0) return cols_ct_launch<T, 0, 2, N, 8>(tin, tout, a, nbox, smem, tiles, st);
+  if (mode == 1) return cols_ct_launch<T, 1, 2, N, 8>(tin, tout, a, nbox, smem, tiles, st);
+  if (dim == 2) return cols_ct_launch<T, 2, 2, N, 12>(tin, tout, a, nbox, smem, tiles, st);
+  return cols_ct_launch<T, 2, 3, N, 12>(tin, tout, a, nbox, smem, tiles, st);
 }
 
 template <typename T, int MODE, int DIM>
@@ -1122,6 +1267,14 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
         b.W = Wp;
         const int thr = tile_threads(Wp);
         const int64_t tiles = (inner + Wp - 1) / Wp * outer;
+        const bool ct_w = Wp == (mode == 2 ? 12 : 8) && (mode != 2 || C == 3 || C == 6);
+        if (ct_w && !getenv("JB_NO_CT")) {
+          if (n == 64) return cols_ct_dispatch<T, 64>(mode, dim, tin, tout, b, nbox, sp, tiles, st);
+          if (n == 128)
+            return cols_ct_dispatch<T, 128>(mode, dim, tin, tout, b, nbox, sp, tiles, st);
+          if (n == 256)
+            return cols_ct_dispatch<T, 256>(mode, dim, tin, tout, b, nbox, sp, tiles, st);
+        }
         if (mode == 0) return cols_tma_launch<T, 0, 2>(tin, tout, b, nbox, thr, sp, tiles, st);
         if (mode == 1) return cols_tma_launch<T, 1, 2>(tin, tout, b, nbox, thr, sp, tiles, st);
         if (dim == 2) return cols_tma_launch<T, 2, 2>(tin, tout, b, nbox, thr, sp, tiles, st);
