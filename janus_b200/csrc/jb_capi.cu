@@ -254,6 +254,8 @@ struct jb_green_s {
   std::vector<void*> tables;
   DeviceBuf spec;
   DeviceBuf bidx;
+  DeviceBuf mnbuf;        // per-coefficient M/N table, built on first use
+  bool use_table = true;  // false: evaluate the operator on the fly
 };
 
 struct jb_local_s {
@@ -360,6 +362,15 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
     rec->mark(st);
   }
   const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
+  if (g->use_table && !g->gt.mn) {
+    // the operator's M/N tensors at every half-spectrum coefficient, once
+    const int NT = dim == 3 ? 21 : 8;
+    const size_t bytes = (size_t)n0 * (dim == 3 ? n1 * m : m) * NT * real_size(g->dtype);
+    JB_TRY(ensure_buf(g->mnbuf, bytes));
+    JB_TRY(launch_status(jb::launch_green_table(g->dtype, dim, g->gt, n0, n1, m, g->mnbuf.p, st),
+                         "green_table"));
+    g->gt.mn = g->mnbuf.p;
+  }
   JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
                                        &g->gt, n1, m, st),
                        "cols_green_axis0"));
@@ -628,6 +639,7 @@ int jb_green_destroy(jb_green* G) {
   for (void* p : G->tables) cudaFree(p);
   if (G->spec.p) cudaFree(G->spec.p);
   if (G->bidx.p) cudaFree(G->bidx.p);
+  if (G->mnbuf.p) cudaFree(G->mnbuf.p);
   delete G;
   return JB_OK;
 }
@@ -1097,6 +1109,7 @@ extern "C" int jb_green_apply_noalloc(int dim, const int64_t* shape, double h, d
   // a stack-held operator description whose device pointers all point into
   // the static array (no handle, no allocation)
   jb_green G;
+  G.use_table = false;  // evaluate the operator on the fly: nothing to allocate
   G.dim = dim;
   G.dtype = F64;
   G.variant = variant;

@@ -20,7 +20,7 @@ template <> struct CtSched<1024> { static constexpr int R0 = 16, R1 = 8, R2 = 8;
 
 // threads of a compile-time tile: the largest butterfly count of a stage,
 // rounded up to whole warps
-template <int N, int W> constexpr int ct_threads() {
+template <int N, int W> __host__ __device__ constexpr int ct_threads() {
   using S = CtSched<N>;
   int m = (N / S::R0) * W;
   if ((N / S::R1) * W > m) m = (N / S::R1) * W;

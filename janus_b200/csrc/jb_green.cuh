@@ -24,6 +24,10 @@
 
 namespace jb {
 
+// correctly rounded reciprocals (same result as 1/x, cheaper than a division)
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+
 template <typename T> struct GreenTables {
   // truncated: kt[d][b]; filtered: kn/kp/wn/wp[d][b] (b < n_d)
   const T* kt[3];
@@ -42,7 +46,7 @@ __device__ __forceinline__ void gamma3_acc(T k0, T k1, T k2, T w, const C* t, C*
                                            T inv2g, T c1) {
   const T kk = k0 * k0 + k1 * k1 + k2 * k2;
   if (kk == T(0)) return;
-  const T q = T(1) / kk;
+  const T q = rcp_rn(kk);
   const T al = q * inv2g * w;
   const T u = T(0.70710678118654752440084436210485);
   const T s2 = T(1.4142135623730950488016887242097);
@@ -81,7 +85,7 @@ __device__ __forceinline__ void gamma2_acc(T k0, T k1, T w, const C* t, C* acc, 
                                            T c1) {
   const T kk = k0 * k0 + k1 * k1;
   if (kk == T(0)) return;
-  const T q = T(1) / kk;
+  const T q = rcp_rn(kk);
   const T al = q * inv2g * w;
   const T u = T(0.70710678118654752440084436210485);
   const T s2 = T(1.4142135623730950488016887242097);
@@ -120,7 +124,7 @@ __device__ __forceinline__ void batch_reciprocal(T* x) {
     pre[0] = x[0];
 #pragma unroll
     for (int i = 1; i < NA; ++i) pre[i] = pre[i - 1] * x[i];
-    T inv = T(1) / pre[NA - 1];
+    T inv = rcp_rn(pre[NA - 1]);
 #pragma unroll
     for (int i = NA - 1; i > 0; --i) {
       const T xi = x[i];
@@ -130,15 +134,16 @@ __device__ __forceinline__ void batch_reciprocal(T* x) {
     x[0] = inv;
   } else {
 #pragma unroll
-    for (int i = 0; i < NA; ++i) x[i] = T(1) / x[i];
+    for (int i = 0; i < NA; ++i) x[i] = rcp_rn(x[i]);
   }
 }
 
+// kx/wx, ky/wy, kz/wz: the two aliases (b - n, b) of each axis and their
+// cos^2 weights
 template <typename T, typename C>
-__device__ __forceinline__ void green_filtered3(const GreenTables<T>& g, const int* b, C* te) {
-  const T kx[2] = {g.kn[0][b[0]], g.kp[0][b[0]]}, wx[2] = {g.wn[0][b[0]], g.wp[0][b[0]]};
-  const T ky[2] = {g.kn[1][b[1]], g.kp[1][b[1]]}, wy[2] = {g.wn[1][b[1]], g.wp[1][b[1]]};
-  const T kz[2] = {g.kn[2][b[2]], g.kp[2][b[2]]}, wz[2] = {g.wn[2][b[2]], g.wp[2][b[2]]};
+__device__ __forceinline__ void green_filtered3(const T* kx, const T* wx, const T* ky,
+                                                const T* wy, const T* kz, const T* wz, T inv2g,
+                                                T c1, C* te) {
   T q[8];
   bool zero[8];
 #pragma unroll
@@ -158,8 +163,8 @@ __device__ __forceinline__ void green_filtered3(const GreenTables<T>& g, const i
     if (zero[a]) continue;
     const T k0 = kx[a >> 2], k1 = ky[(a >> 1) & 1], k2 = kz[a & 1];
     const T w = wx[a >> 2] * wy[(a >> 1) & 1] * wz[a & 1];
-    const T al = w * q[a] * g.inv2g;
-    const T be = al * q[a] * g.c1;
+    const T al = w * q[a] * inv2g;
+    const T be = al * q[a] * c1;
     const T p00 = k0 * k0, p11 = k1 * k1, p22 = k2 * k2;
     const T p12 = k1 * k2, p20 = k2 * k0, p01 = k0 * k1;
     m00 += al * p00; m11 += al * p11; m22 += al * p22;
@@ -204,9 +209,8 @@ __device__ __forceinline__ void green_filtered3(const GreenTables<T>& g, const i
 }
 
 template <typename T, typename C>
-__device__ __forceinline__ void green_filtered2(const GreenTables<T>& g, const int* b, C* te) {
-  const T kx[2] = {g.kn[0][b[0]], g.kp[0][b[0]]}, wx[2] = {g.wn[0][b[0]], g.wp[0][b[0]]};
-  const T ky[2] = {g.kn[1][b[1]], g.kp[1][b[1]]}, wy[2] = {g.wn[1][b[1]], g.wp[1][b[1]]};
+__device__ __forceinline__ void green_filtered2(const T* kx, const T* wx, const T* ky,
+                                                const T* wy, T inv2g, T c1, C* te) {
   T q[4];
   bool zero[4];
 #pragma unroll
@@ -223,8 +227,8 @@ __device__ __forceinline__ void green_filtered2(const GreenTables<T>& g, const i
     if (zero[a]) continue;
     const T k0 = kx[a >> 1], k1 = ky[a & 1];
     const T w = wx[a >> 1] * wy[a & 1];
-    const T al = w * q[a] * g.inv2g;
-    const T be = al * q[a] * g.c1;
+    const T al = w * q[a] * inv2g;
+    const T be = al * q[a] * c1;
     const T p00 = k0 * k0, p11 = k1 * k1, p01 = k0 * k1;
     m00 += al * p00; m11 += al * p11; m01 += al * p01;
     const T b00 = be * p00, b11 = be * p11;
@@ -252,33 +256,208 @@ __device__ __forceinline__ void green_filtered2(const GreenTables<T>& g, const i
   }
 }
 
-// eta = Gamma_discrete(b) : tau for one half-spectrum index b (b[d] < n_d).
-// tau and eta may alias.
+// ---------------------------------------------------------------------------
+// Tabulated form: per half-spectrum coefficient the tensors M (sym. rank 2)
+// and N (fully sym. rank 4) of  Gamma_discrete:t = M t + t M - N:t  (with the
+// 1/(2g) and 1/(1-nu) factors folded in).  Truncated = one alias, filtered =
+// the 2^d-alias sums.  3D: 21 reals [m00 m11 m22 m12 m20 m01 | n400 n040 n004
+// n220 n202 n022 n310 n301 n130 n031 n103 n013 n211 n121 n112]; 2D: 8 reals
+// [m00 m11 m01 | n40 n31 n22 n13 n04].
+// ---------------------------------------------------------------------------
+template <int DIM> struct MnSize;
+template <> struct MnSize<2> { static constexpr int value = 8; };
+template <> struct MnSize<3> { static constexpr int value = 21; };
+
+template <typename T>
+__device__ __forceinline__ void mn_accumulate3(T k0, T k1, T k2, T al, T be, T* mn) {
+  const T p00 = k0 * k0, p11 = k1 * k1, p22 = k2 * k2;
+  const T p12 = k1 * k2, p20 = k2 * k0, p01 = k0 * k1;
+  mn[0] += al * p00; mn[1] += al * p11; mn[2] += al * p22;
+  mn[3] += al * p12; mn[4] += al * p20; mn[5] += al * p01;
+  const T b00 = be * p00, b11 = be * p11, b22 = be * p22;
+  mn[6] += b00 * p00; mn[7] += b11 * p11; mn[8] += b22 * p22;
+  mn[9] += b00 * p11; mn[10] += b00 * p22; mn[11] += b11 * p22;
+  mn[12] += b00 * p01; mn[13] += b00 * p20; mn[14] += b11 * p01;
+  mn[15] += b11 * p12; mn[16] += b22 * p20; mn[17] += b22 * p12;
+  mn[18] += b00 * p12; mn[19] += b11 * p20; mn[20] += b22 * p01;
+}
+
+template <typename T>
+__device__ __forceinline__ void mn_accumulate2(T k0, T k1, T al, T be, T* mn) {
+  const T p00 = k0 * k0, p11 = k1 * k1, p01 = k0 * k1;
+  mn[0] += al * p00; mn[1] += al * p11; mn[2] += al * p01;
+  const T b00 = be * p00, b11 = be * p11;
+  mn[3] += b00 * p00; mn[4] += b00 * p01; mn[5] += b00 * p11; mn[6] += b11 * p01;
+  mn[7] += b11 * p11;
+}
+
+// M/N of one coefficient from its per-axis values (AxisK: truncated k in
+// v[0]; filtered k-, k+, w-, w+)
+template <int DIM, typename T>
+__device__ __forceinline__ void mn_build(int variant, const T* a0, const T* a1, const T* a2,
+                                         T inv2g, T c1, T* mn) {
+  constexpr int NT = MnSize<DIM>::value;
+#pragma unroll
+  for (int i = 0; i < NT; ++i) mn[i] = T(0);
+  constexpr int NA = DIM == 3 ? 8 : 4;
+  const int na = variant == 0 ? 1 : NA;
+  for (int a = 0; a < na; ++a) {
+    T k0, k1, k2 = T(0), w;
+    if (variant == 0) {
+      k0 = a0[0];
+      k1 = a1[0];
+      if (DIM == 3) k2 = a2[0];
+      w = T(1);
+    } else if (DIM == 3) {
+      const int s0 = a >> 2, s1 = (a >> 1) & 1, s2 = a & 1;
+      k0 = a0[s0];
+      k1 = a1[s1];
+      k2 = a2[s2];
+      w = a0[2 + s0] * a1[2 + s1] * a2[2 + s2];
+    } else {
+      const int s0 = a >> 1, s1 = a & 1;
+      k0 = a0[s0];
+      k1 = a1[s1];
+      w = a0[2 + s0] * a1[2 + s1];
+    }
+    const T kk = k0 * k0 + k1 * k1 + k2 * k2;
+    if (kk == T(0)) continue;
+    const T q = rcp_rn(kk);
+    const T al = w * q * inv2g;
+    const T be = al * q * c1;
+    if (DIM == 3)
+      mn_accumulate3(k0, k1, k2, al, be, mn);
+    else
+      mn_accumulate2(k0, k1, al, be, mn);
+  }
+}
+
+// te <- M te + te M - N:te (Mandel, real and imaginary parts)
+template <int DIM, typename T, typename C>
+__device__ __forceinline__ void mn_apply(const T* mn, C* te) {
+  const T u = T(0.70710678118654752440084436210485);
+  const T s2 = T(1.4142135623730950488016887242097);
+  if (DIM == 3) {
+    const T m00 = mn[0], m11 = mn[1], m22 = mn[2], m12 = mn[3], m20 = mn[4], m01 = mn[5];
+    const T n400 = mn[6], n040 = mn[7], n004 = mn[8], n220 = mn[9], n202 = mn[10],
+            n022 = mn[11], n310 = mn[12], n301 = mn[13], n130 = mn[14], n031 = mn[15],
+            n103 = mn[16], n013 = mn[17], n211 = mn[18], n121 = mn[19], n112 = mn[20];
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      const T t00 = part ? te[0].y : te[0].x;
+      const T t11 = part ? te[1].y : te[1].x;
+      const T t22 = part ? te[2].y : te[2].x;
+      const T t12 = u * (part ? te[3].y : te[3].x);
+      const T t20 = u * (part ? te[4].y : te[4].x);
+      const T t01 = u * (part ? te[5].y : te[5].x);
+      const T S00 = n400 * t00 + n220 * t11 + n202 * t22 + T(2) * (n211 * t12 + n301 * t20 + n310 * t01);
+      const T S11 = n220 * t00 + n040 * t11 + n022 * t22 + T(2) * (n031 * t12 + n121 * t20 + n130 * t01);
+      const T S22 = n202 * t00 + n022 * t11 + n004 * t22 + T(2) * (n013 * t12 + n103 * t20 + n112 * t01);
+      const T S12 = n211 * t00 + n031 * t11 + n013 * t22 + T(2) * (n022 * t12 + n112 * t20 + n121 * t01);
+      const T S20 = n301 * t00 + n121 * t11 + n103 * t22 + T(2) * (n112 * t12 + n202 * t20 + n211 * t01);
+      const T S01 = n310 * t00 + n130 * t11 + n112 * t22 + T(2) * (n121 * t12 + n211 * t20 + n220 * t01);
+      const T P00 = T(2) * (m00 * t00 + m01 * t01 + m20 * t20);
+      const T P11 = T(2) * (m01 * t01 + m11 * t11 + m12 * t12);
+      const T P22 = T(2) * (m20 * t20 + m12 * t12 + m22 * t22);
+      const T P12 = (m11 + m22) * t12 + m12 * (t11 + t22) + m01 * t20 + m20 * t01;
+      const T P20 = (m22 + m00) * t20 + m20 * (t22 + t00) + m12 * t01 + m01 * t12;
+      const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11) + m20 * t12 + m12 * t20;
+      const T o0 = P00 - S00, o1 = P11 - S11, o2 = P22 - S22;
+      const T o3 = s2 * (P12 - S12), o4 = s2 * (P20 - S20), o5 = s2 * (P01 - S01);
+      if (part == 0) {
+        te[0].x = o0; te[1].x = o1; te[2].x = o2; te[3].x = o3; te[4].x = o4; te[5].x = o5;
+      } else {
+        te[0].y = o0; te[1].y = o1; te[2].y = o2; te[3].y = o3; te[4].y = o4; te[5].y = o5;
+      }
+    }
+  } else {
+    const T m00 = mn[0], m11 = mn[1], m01 = mn[2];
+    const T n40 = mn[3], n31 = mn[4], n22 = mn[5], n13 = mn[6], n04 = mn[7];
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      const T t00 = part ? te[0].y : te[0].x;
+      const T t11 = part ? te[1].y : te[1].x;
+      const T t01 = u * (part ? te[2].y : te[2].x);
+      const T S00 = n40 * t00 + n22 * t11 + T(2) * n31 * t01;
+      const T S11 = n22 * t00 + n04 * t11 + T(2) * n13 * t01;
+      const T S01 = n31 * t00 + n13 * t11 + T(2) * n22 * t01;
+      const T P00 = T(2) * (m00 * t00 + m01 * t01);
+      const T P11 = T(2) * (m01 * t01 + m11 * t11);
+      const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11);
+      const T o0 = P00 - S00, o1 = P11 - S11, o2 = s2 * (P01 - S01);
+      if (part == 0) {
+        te[0].x = o0; te[1].x = o1; te[2].x = o2;
+      } else {
+        te[0].y = o0; te[1].y = o1; te[2].y = o2;
+      }
+    }
+  }
+}
+
+// Per-axis values of one index b_d: truncated k (slot 0) or the filtered
+// aliases (k-, k+, w-, w+).
+template <typename T> struct AxisK {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ AxisK<T> axis_values(const GreenTables<T>& g, int d, int bd) {
+  AxisK<T> r;
+  if (g.variant == 0) {
+    r.v[0] = g.kt[d][bd];
+    r.v[1] = r.v[2] = r.v[3] = T(0);
+  } else {
+    r.v[0] = g.kn[d][bd];
+    r.v[1] = g.kp[d][bd];
+    r.v[2] = g.wn[d][bd];
+    r.v[3] = g.wp[d][bd];
+  }
+  return r;
+}
+
+// eta = Gamma_discrete : tau for one half-spectrum coefficient whose per-axis
+// values are given (a1 unused in 2D).  tau and eta alias.
+template <int DIM, typename T, typename C>
+__device__ __forceinline__ void green_contract_k(int variant, const AxisK<T>& a0,
+                                                 const AxisK<T>& a1, const AxisK<T>& a2,
+                                                 T inv2g, T c1, C* te) {
+  constexpr int S = DIM == 2 ? 3 : 6;
+  C t[S];
+#pragma unroll
+  for (int i = 0; i < S; ++i) t[i] = te[i];
+  if (variant == 0) {
+    C acc[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) acc[i] = mkc(T(0), T(0));
+    if (DIM == 2)
+      gamma2_acc(a0.v[0], a1.v[0], T(1), t, acc, inv2g, c1);
+    else
+      gamma3_acc(a0.v[0], a1.v[0], a2.v[0], T(1), t, acc, inv2g, c1);
+#pragma unroll
+    for (int i = 0; i < S; ++i) te[i] = acc[i];
+  } else {
+    const T kx[2] = {a0.v[0], a0.v[1]}, wx[2] = {a0.v[2], a0.v[3]};
+    const T ky[2] = {a1.v[0], a1.v[1]}, wy[2] = {a1.v[2], a1.v[3]};
+    if (DIM == 2) {
+      green_filtered2<T>(kx, wx, ky, wy, inv2g, c1, t);
+    } else {
+      const T kz[2] = {a2.v[0], a2.v[1]}, wz[2] = {a2.v[2], a2.v[3]};
+      green_filtered3<T>(kx, wx, ky, wy, kz, wz, inv2g, c1, t);
+    }
+#pragma unroll
+    for (int i = 0; i < S; ++i) te[i] = t[i];
+  }
+}
+
+// eta = Gamma_discrete(b) : tau for one half-spectrum index b (b[d] < n_d),
+// reading the per-axis tables from global memory.  tau and eta may alias.
 template <int DIM, typename T, typename C>
 __device__ __forceinline__ void green_contract(const GreenTables<T>& g, const int* b,
                                                C* tau_eta) {
-  constexpr int S = DIM == 2 ? 3 : 6;
-  C t[S], acc[S];
-#pragma unroll
-  for (int i = 0; i < S; ++i) {
-    t[i] = tau_eta[i];
-    acc[i] = mkc(T(0), T(0));
-  }
-  if (g.variant == 0) {
-    if (DIM == 2)
-      gamma2_acc(g.kt[0][b[0]], g.kt[1][b[1]], T(1), t, acc, g.inv2g, g.c1);
-    else
-      gamma3_acc(g.kt[0][b[0]], g.kt[1][b[1]], g.kt[2][b[2]], T(1), t, acc, g.inv2g, g.c1);
-  } else {
-    if (DIM == 2)
-      green_filtered2<T>(g, b, t);
-    else
-      green_filtered3<T>(g, b, t);
-#pragma unroll
-    for (int i = 0; i < S; ++i) acc[i] = t[i];
-  }
-#pragma unroll
-  for (int i = 0; i < S; ++i) tau_eta[i] = acc[i];
+  const AxisK<T> a0 = axis_values(g, 0, b[0]);
+  const AxisK<T> a1 = axis_values(g, 1, b[1]);
+  const AxisK<T> a2 = DIM == 3 ? axis_values(g, 2, b[2]) : a1;
+  green_contract_k<DIM, T>(g.variant, a0, a1, a2, g.inv2g, g.c1, tau_eta);
 }
 
 }  // namespace jb

@@ -141,7 +141,7 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* fail_flag) {
 template <typename T, int CC, bool LOCAL, int NCT = 0, int WCT = 0>
 __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
   using C = cx<T>;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int fail_flag;
   const int n = NCT > 0 ? NCT : a.plan.n;
@@ -272,7 +272,7 @@ template <typename T, int CC, int EPI, int NCT = 0, int WCT = 0>
 __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   using OT = typename std::conditional<EPI == kEpiResid, float, T>::type;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int fail_flag;
   __shared__ double red[kThreads / 32];
@@ -422,6 +422,7 @@ template <typename T> struct ColsArgs {
   int W, C;
   int64_t m_last;
   GreenTables<T> gt;
+  const T* mn;  // MODE 2: M/N table, or nullptr to evaluate the operator on the fly
 };
 
 // complex transform along a strided axis of [outer][n][inner]: a tile of n
@@ -431,7 +432,7 @@ template <typename T> struct ColsArgs {
 template <typename T, int MODE, int DIM>
 __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
   using C = cx<T>;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int fail_flag;
   const int n = a.plan.n, W = a.W;
@@ -570,6 +571,7 @@ __global__ void __launch_bounds__(kThreads)
   In[0] = align128_ptr<C>(tw + n);
   In[1] = align128_ptr<C>(In[0] + tile);
   C* Wk = align128_ptr<C>(In[1] + tile);
+  AxisK<T>* ax0 = align128_ptr<AxisK<T>>(Wk + tile);  // MODE 2: axis-0 Green values
   const int64_t ntx = (a.inner + W - 1) / W;
   const int64_t total = ntx * a.outer;
   if (threadIdx.x == 0) {
@@ -579,10 +581,24 @@ __global__ void __launch_bounds__(kThreads)
     fence_mbar_init();
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
+  if (MODE == 2)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) ax0[i] = axis_values(a.gt, 0, i);
   __syncthreads();
+  // tile t -> (o, chunk); the Green pass walks the load cases of a chunk
+  // consecutively so they share its M/N table slice in L2
+  auto tile_of = [&](int64_t t, int64_t& o, int64_t& chunk) {
+    if (MODE == 2) {
+      chunk = t / a.outer;
+      o = t - chunk * a.outer;
+    } else {
+      o = t / ntx;
+      chunk = t - o * ntx;
+    }
+  };
   auto issue_load = [&](int64_t t, C* dst, uint64_t* b) {
-    const int64_t o = t / ntx;
-    const int x = (int)(2 * (t - o * ntx) * W);
+    int64_t o, chunk;
+    tile_of(t, o, chunk);
+    const int x = (int)(2 * chunk * W);
     mbar_arrive_expect_tx(b, (uint32_t)(tile * sizeof(C)));
     for (int yb = 0; yb < n; yb += nbox) tma_load_3d(dst + (size_t)yb * W, &tin, x, yb, (int)o, b);
   };
@@ -591,8 +607,9 @@ __global__ void __launch_bounds__(kThreads)
   const Lane ln = make_lane(W);
   for (int i = 0; t < total; ++i, t += gridDim.x) {
     const int buf = i & 1;
-    const int64_t o = t / ntx;
-    const int64_t c0 = (t - o * ntx) * W;
+    int64_t o, chunk;
+    tile_of(t, o, chunk);
+    const int64_t c0 = chunk * W;
     const int Wc = (int)min((int64_t)W, a.inner - c0);
     C* in = In[buf];
     if (!mbar_wait(&bar[buf], (i >> 1) & 1)) atomicOr(&fail_flag, 1);
@@ -624,17 +641,29 @@ __global__ void __launch_bounds__(kThreads)
         const int col0 = fl * Cc;
         if (col0 < Wc) {
           const int64_t f = (c0 + col0) / Cc;
-          int b[3];
+          int b1, b2;
           if (DIM == 3) {
-            b[1] = (int)(f / a.m_last);
-            b[2] = (int)(f % a.m_last);
+            b1 = (int)(f / a.m_last);
+            b2 = (int)(f % a.m_last);
           } else {
-            b[1] = (int)f;
-            b[2] = 0;
+            b1 = (int)f;
+            b2 = 0;
           }
-          for (int e = e0; e < n; e += est) {
-            b[0] = e;
-            green_contract<DIM, T>(a.gt, b, Z + e * W + col0);
+          if (a.mn != nullptr) {
+            constexpr int NT = MnSize<DIM>::value;
+            const T* tab = a.mn + (size_t)f * n * NT;
+            for (int e = e0; e < n; e += est) {
+              T mn[NT];
+#pragma unroll
+              for (int c = 0; c < NT; ++c) mn[c] = __ldg(tab + (size_t)e * NT + c);
+              mn_apply<DIM, T>(mn, Z + e * W + col0);
+            }
+          } else {
+            const AxisK<T> a1 = axis_values(a.gt, 1, b1);
+            const AxisK<T> a2 = DIM == 3 ? axis_values(a.gt, 2, b2) : a1;
+            for (int e = e0; e < n; e += est)
+              green_contract_k<DIM, T>(a.gt.variant, ax0[e], a1, a2, a.gt.inv2g, a.gt.c1,
+                                       Z + e * W + col0);
           }
         }
       }
@@ -755,6 +784,33 @@ __global__ void convert_f64_to_f32_kernel(int64_t n, const double* __restrict__ 
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     y[i] = static_cast<float>(x[i]);
+}
+
+template <typename T, int DIM>
+__global__ void green_table_kernel(GreenTables<T> gt, int64_t n0, int64_t n1, int64_t m_last,
+                                   T* out) {
+  constexpr int NT = MnSize<DIM>::value;
+  const int64_t f12n = DIM == 3 ? n1 * m_last : m_last;
+  const int64_t total = f12n * n0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t f = i / n0;
+    const int b0 = (int)(i - f * n0);
+    int b1, b2 = 0;
+    if (DIM == 3) {
+      b1 = (int)(f / m_last);
+      b2 = (int)(f - (int64_t)b1 * m_last);
+    } else {
+      b1 = (int)f;
+    }
+    const AxisK<T> a0 = axis_values(gt, 0, b0);
+    const AxisK<T> a1 = axis_values(gt, 1, b1);
+    const AxisK<T> a2 = DIM == 3 ? axis_values(gt, 2, b2) : a1;
+    T mn[NT];
+    mn_build<DIM, T>(gt.variant, a0.v, a1.v, a2.v, gt.inv2g, gt.c1, mn);
+#pragma unroll
+    for (int c = 0; c < NT; ++c) out[i * NT + c] = mn[c];
+  }
 }
 
 template <typename T>
@@ -913,7 +969,8 @@ bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem) {
   }
   if (w < unit) w = unit;
   for (;; w -= unit) {
-    const size_t bytes = n * cs + 3 * 128 + 3 * (size_t)n * w * cs;
+    // + the axis-0 Green values (4 reals per row) and alignment
+    const size_t bytes = n * cs + 4 * 128 + 3 * (size_t)n * w * cs + (size_t)n * 2 * cs;
     if (bytes <= kPipeBudget || w <= unit) {
       if (bytes > kSmemCap - 4096 || (w * cs) % 16 != 0) return false;
       *W = w;
@@ -1250,6 +1307,7 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
   a.C = C;
   a.m_last = m_last;
   a.gt = to_tables<T>(gt);
+  a.mn = gt ? static_cast<const T*>(gt->mn) : nullptr;
   a.outer = outer;
   {
     int Wp;
@@ -1389,6 +1447,30 @@ cudaError_t launch_green_by_freq(int dtype, int dim, const GreenDeviceTables& gt
     else
       green_by_freq_kernel<float, 3><<<grid, kThreads, 0, st>>>(
           t, count, b, static_cast<const float2*>(tau), static_cast<float2*>(eta));
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_green_table(int dtype, int dim, const GreenDeviceTables& gt, int64_t n0,
+                               int64_t n1, int64_t m_last, void* out, cudaStream_t st) {
+  const int64_t total = (dim == 3 ? n1 * m_last : m_last) * n0;
+  const int grid = grid_for(total);
+  if (dtype == F64) {
+    auto t = to_tables<double>(&gt);
+    if (dim == 2)
+      green_table_kernel<double, 2><<<grid, kThreads, 0, st>>>(t, n0, n1, m_last,
+                                                                 static_cast<double*>(out));
+    else
+      green_table_kernel<double, 3><<<grid, kThreads, 0, st>>>(t, n0, n1, m_last,
+                                                                 static_cast<double*>(out));
+  } else {
+    auto t = to_tables<float>(&gt);
+    if (dim == 2)
+      green_table_kernel<float, 2><<<grid, kThreads, 0, st>>>(t, n0, n1, m_last,
+                                                                static_cast<float*>(out));
+    else
+      green_table_kernel<float, 3><<<grid, kThreads, 0, st>>>(t, n0, n1, m_last,
+                                                                static_cast<float*>(out));
   }
   return cudaGetLastError();
 }

@@ -27,6 +27,7 @@ struct GreenDeviceTables {
   void* wp[3] = {nullptr, nullptr, nullptr};
   double inv2g = 0, c1 = 0;
   int variant = 0;
+  const void* mn = nullptr;  // per-coefficient M/N table (T), built by launch_green_table
 };
 
 // Real-side geometry of a batch of fields [L][rows][n][C] with arbitrary
@@ -86,6 +87,11 @@ cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer,
                         int64_t inner, const void* in, void* out, int C, int dim,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
                         cudaStream_t st);
+// M/N table of the Green operator on the half spectrum of an n0 x n1 (x n2)
+// grid: table[(f12 * n0 + b0) * NT + c], f12 = b1 * m + b2 (3D) or b1 (2D),
+// NT = 21 (3D) / 8 (2D).  `out` has n0 * n1 * m * NT (3D) reals of the dtype.
+cudaError_t launch_green_table(int dtype, int dim, const GreenDeviceTables& gt, int64_t n0,
+                               int64_t n1, int64_t m_last, void* out, cudaStream_t st);
 // y[l][v] = (C - C0)(v) : x[l][v] on a phase map (contiguous fields)
 cudaError_t launch_local(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
                          const void* x, void* y, cudaStream_t st);
