@@ -88,6 +88,11 @@ __device__ __forceinline__ void bulk_wait_read() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// the same, for all but the most recently committed group
+__device__ __forceinline__ void bulk_wait_read_1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+
 // order this thread's generic-proxy shared-memory writes before later
 // async-proxy (bulk copy) accesses
 __device__ __forceinline__ void fence_async_shared() {

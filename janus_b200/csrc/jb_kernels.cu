@@ -423,6 +423,7 @@ template <typename T> struct ColsArgs {
   int64_t m_last;
   GreenTables<T> gt;
   const T* mn;  // MODE 2: M/N table, or nullptr to evaluate the operator on the fly
+  int nbuf;     // tensor-TMA kernel: rotating input tiles (2 or 3)
 };
 
 // complex transform along a strided axis of [outer][n][inner]: a tile of n
@@ -555,22 +556,39 @@ template <typename P> __device__ __forceinline__ P* align128_ptr(void* p) {
 // tile is computed, and stored back as boxes from shared memory.  Columns
 // past `inner` in the last chunk are zero-filled by the load and skipped by
 // the store.  Persistent grid; thread 0 issues all copies.
+// resident CTAs per SM the Green pass asks the register allocator for
+// (register pressure, not shared memory, bounded its occupancy)
+template <typename T, int MODE, int NCT> constexpr int cols_min_blocks() {
+  return (MODE == 2 && NCT > 0) ? (sizeof(T) == 8 ? 2 : 4) : 1;
+}
+template <int NCT, int WCT> constexpr int cols_max_threads() {
+  if constexpr (NCT > 0)
+    return ct_threads<NCT, WCT>();
+  else
+    return kThreads;
+}
+
 template <typename T, int MODE, int DIM, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(cols_max_threads<NCT, WCT>(), cols_min_blocks<T, MODE, NCT>())
     cols_tma_kernel(const __grid_constant__ CUtensorMap tin,
                     const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar[3];
   __shared__ int fail_flag;
   const int n = NCT > 0 ? NCT : a.plan.n;
   const int W = WCT > 0 ? WCT : a.W;
+  const int nbuf = a.nbuf;
   const size_t tile = (size_t)n * W;
   C* tw = reinterpret_cast<C*>(smem);
-  C* In[2];
-  In[0] = align128_ptr<C>(tw + n);
-  In[1] = align128_ptr<C>(In[0] + tile);
-  C* Wk = align128_ptr<C>(In[1] + tile);
+  // input tiles rotate so that the tile a load overwrites was stored an
+  // iteration earlier with three of them: its store has drained by then
+  C* const In0 = align128_ptr<C>(tw + n);
+  const size_t tstride = (tile * sizeof(C) + 127) / 128 * 128;  // bytes between input tiles
+  auto in_tile = [&](int b) {
+    return reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(In0) + b * tstride);
+  };
+  C* Wk = in_tile(nbuf);
   AxisK<T>* ax0 = align128_ptr<AxisK<T>>(Wk + tile);  // MODE 2: axis-0 Green values
   const int64_t ntx = (a.inner + W - 1) / W;
   const int64_t total = ntx * a.outer;
@@ -578,10 +596,11 @@ __global__ void __launch_bounds__(kThreads)
     fail_flag = 0;
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
     fence_mbar_init();
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
-  if (MODE == 2)
+  if (MODE == 2 && a.mn == nullptr)
     for (int i = threadIdx.x; i < n; i += blockDim.x) ax0[i] = axis_values(a.gt, 0, i);
   __syncthreads();
   // tile t -> (o, chunk); the Green pass walks the load cases of a chunk
@@ -603,21 +622,32 @@ __global__ void __launch_bounds__(kThreads)
     for (int yb = 0; yb < n; yb += nbox) tma_load_3d(dst + (size_t)yb * W, &tin, x, yb, (int)o, b);
   };
   int64_t t = blockIdx.x;
-  if (t < total && threadIdx.x == 0) issue_load(t, In[0], &bar[0]);
+  if (t < total && threadIdx.x == 0) issue_load(t, In0, &bar[0]);
   const Lane ln = make_lane(W);
-  for (int i = 0; t < total; ++i, t += gridDim.x) {
-    const int buf = i & 1;
+  bool stored_wk = false;  // the last store read the partner tile Wk
+  for (int i = 0, buf = 0, use = 0; t < total; ++i, t += gridDim.x) {
     int64_t o, chunk;
     tile_of(t, o, chunk);
     const int64_t c0 = chunk * W;
     const int Wc = (int)min((int64_t)W, a.inner - c0);
-    C* in = In[buf];
-    if (!mbar_wait(&bar[buf], (i >> 1) & 1)) atomicOr(&fail_flag, 1);
-    if (threadIdx.x == 0) bulk_wait_read();  // the previous tile's stores have read smem
+    C* in = in_tile(buf);
+    if (!mbar_wait(&bar[buf], use & 1)) atomicOr(&fail_flag, 1);
+    // the store that read the next buffer: the previous tile's with two
+    // buffers, the one before it with three (at most one group pending);
+    // all of them when the last store read Wk, which this tile rewrites
+    if (threadIdx.x == 0) {
+      if (nbuf > 2 && !stored_wk)
+        bulk_wait_read_1();
+      else
+        bulk_wait_read();
+    }
     __syncthreads();
     if (fail_flag) return;
     const int64_t tn = t + gridDim.x;
-    if (threadIdx.x == 0 && tn < total) issue_load(tn, In[buf ^ 1], &bar[buf ^ 1]);
+    const int nb = buf + 1 == nbuf ? 0 : buf + 1;
+    if (threadIdx.x == 0 && tn < total) issue_load(tn, in_tile(nb), &bar[nb]);
+    use += nb == 0;
+    buf = nb;
     C* Z;
     if constexpr (NCT > 0) {
       if (MODE == 1)
@@ -655,7 +685,7 @@ __global__ void __launch_bounds__(kThreads)
             for (int e = e0; e < n; e += est) {
               T mn[NT];
 #pragma unroll
-              for (int c = 0; c < NT; ++c) mn[c] = __ldg(tab + (size_t)e * NT + c);
+              for (int c = 0; c < NT; ++c) mn[c] = __ldg(tab + (size_t)c * n + e);
               mn_apply<DIM, T>(mn, Z + e * W + col0);
             }
           } else {
@@ -676,6 +706,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     fence_async_shared();
     __syncthreads();
+    stored_wk = Z == Wk;
     if (threadIdx.x == 0) {
       const int x = (int)(2 * c0);
       for (int yb = 0; yb < n; yb += nbox) tma_store_3d(&tout, x, yb, (int)o, Z + (size_t)yb * W);
@@ -809,7 +840,7 @@ __global__ void green_table_kernel(GreenTables<T> gt, int64_t n0, int64_t n1, in
     T mn[NT];
     mn_build<DIM, T>(gt.variant, a0.v, a1.v, a2.v, gt.inv2g, gt.c1, mn);
 #pragma unroll
-    for (int c = 0; c < NT; ++c) out[i * NT + c] = mn[c];
+    for (int c = 0; c < NT; ++c) out[(f * NT + c) * n0 + b0] = mn[c];
   }
 }
 
@@ -958,7 +989,8 @@ int persistent_grid(K kernel, int threads, size_t smem, int64_t tiles) {
 
 // tile width and shared memory of the tensor-TMA column kernel: two input
 // tiles and one compute partner of n x W complex, 128-byte aligned
-bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem) {
+bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem, int* nbuf,
+                    bool stage_ax0 = true) {
   const size_t cs = dtype == F64 ? 16 : 8;
   // measured on B200 (128^3 x 6, FP64): W = 8 columns for plain passes,
   // 12 (two 6-component coefficients) for the Green pass
@@ -969,12 +1001,23 @@ bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem) {
   }
   if (w < unit) w = unit;
   for (;; w -= unit) {
-    // + the axis-0 Green values (4 reals per row) and alignment
-    const size_t bytes = n * cs + 4 * 128 + 3 * (size_t)n * w * cs + (size_t)n * 2 * cs;
+    // + the axis-0 Green values (4 reals per row, unless tabulated) and alignment
+    auto bytes_for = [&](int nb) {
+      return n * cs + (nb + 1) * 128 + (nb + 1) * (size_t)n * w * cs +
+             (stage_ax0 ? (size_t)n * 2 * cs + 128 : 0);
+    };
+    // a third input tile for FP32, where two CTAs per SM still fit (measured
+    // on B200, 128^3 x 6: FP32 plain passes 8% faster with three; FP64
+    // slower, the third tile costing a resident CTA)
+    int nb = dtype == F32 ? 3 : 2;
+    if (const char* env = getenv("JB_COLS_NBUF")) nb = atoi(env) == 3 ? 3 : 2;
+    if (bytes_for(nb) > kPipeBudget) nb = 2;
+    const size_t bytes = bytes_for(nb);
     if (bytes <= kPipeBudget || w <= unit) {
       if (bytes > kSmemCap - 4096 || (w * cs) % 16 != 0) return false;
       *W = w;
       *smem = bytes;
+      *nbuf = nb;
       return true;
     }
   }
@@ -1310,11 +1353,12 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
   a.mn = gt ? static_cast<const T*>(gt->mn) : nullptr;
   a.outer = outer;
   {
-    int Wp;
+    int Wp, nbuf;
     size_t sp;
     const size_t cs = sizeof(cx<T>);
     if (al16(in) && al16(out) && (inner * cs) % 16 == 0 &&
-        cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &Wp, &sp)) {
+        cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &Wp, &sp, &nbuf,
+                       mode == 2 && a.mn == nullptr)) {
       int nbox = n <= 256 ? n : 256;  // rows per box: largest divisor of n up to 256
       while (n % nbox != 0) --nbox;
       CUtensorMap tin, tout;
@@ -1323,6 +1367,7 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
           make_cols_map(&tout, out, sizeof(T) == 8, inner, n, outer, Wp, nbox)) {
         ColsArgs<T> b = a;
         b.W = Wp;
+        b.nbuf = nbuf;
         const int thr = tile_threads(Wp);
         const int64_t tiles = (inner + Wp - 1) / Wp * outer;
         const bool ct_w = Wp == (mode == 2 ? 12 : 8) && (mode != 2 || C == 3 || C == 6);
