@@ -121,6 +121,56 @@ template <typename P> __device__ __forceinline__ P* align16_ptr(void* p) {
   return reinterpret_cast<P*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
 }
 
+// two-element vectors for 16-byte (FP64) / 8-byte (FP32) shared-memory access
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// padding (reals) after each row of a raw real chunk staged in shared memory
+// by the compile-time row kernels: 32 bytes shift consecutive rows by 8
+// banks, so a warp mapping (row fastest, voxel next) reads and writes the
+// chunk and the FFT tile without bank conflicts.  A tile (n + 2) x W complex
+// holds R rows of n*CC reals plus 2*CC reals of slack per row, so FP32 with
+// CC = 3 takes 16 bytes.
+template <typename T, int CC> constexpr int row_pad() {
+  return (2 * CC * (int)sizeof(T) >= 32 ? 32 : 16) / (int)sizeof(T);
+}
+
+// the CC components of one voxel between shared memory and registers
+// (vector accesses when CC is even)
+template <typename T, int CC>
+__device__ __forceinline__ void load_voxel(const T* __restrict__ src, T (&v)[CC]) {
+  if constexpr (CC % 2 == 0) {
+    using V = typename Vec2<T>::type;
+#pragma unroll
+    for (int j = 0; j < CC / 2; ++j) {
+      const V w = reinterpret_cast<const V*>(src)[j];
+      v[2 * j] = w.x;
+      v[2 * j + 1] = w.y;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < CC; ++c) v[c] = src[c];
+  }
+}
+
+template <typename T, int CC>
+__device__ __forceinline__ void store_voxel(T* __restrict__ dst, const T (&v)[CC]) {
+  if constexpr (CC % 2 == 0) {
+    using V = typename Vec2<T>::type;
+#pragma unroll
+    for (int j = 0; j < CC / 2; ++j) {
+      V w;
+      w.x = v[2 * j];
+      w.y = v[2 * j + 1];
+      reinterpret_cast<V*>(dst)[j] = w;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < CC; ++c) dst[c] = v[c];
+  }
+}
+
 // every thread waits (bounded) on the tile barrier; false if any timed out
 __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* fail_flag) {
   if (!mbar_wait(bar, 0)) atomicOr(fail_flag, 1);
@@ -159,10 +209,13 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
   const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
   constexpr int kC = CC;
   const int RC = R * kC;
+  // raw chunk rows in B, ldb reals apart (padded for the compile-time tiles)
+  const int ldb = n * kC + (NCT > 0 ? row_pad<T, kC>() : 0);
   const T* xl = a.x + l * a.g.ls;
   const T* chunk = xl + row0 * n * kC;
   const uint32_t bytes = (uint32_t)(rows_here * n * kC * sizeof(T));
-  const bool bulk = a.contig && aligned16(chunk) && (bytes % 16 == 0) && aligned16(Br);
+  const uint32_t rbytes = (uint32_t)(n * kC * sizeof(T));
+  const bool bulk = a.contig && aligned16(chunk) && (rbytes % 16 == 0) && aligned16(Br);
   if (threadIdx.x == 0) {
     fail_flag = 0;
     mbar_init(&bar, 1);
@@ -172,14 +225,19 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
   if (bulk) {
     if (threadIdx.x == 0) {
       mbar_arrive_expect_tx(&bar, bytes);
-      bulk_load(Br, chunk, bytes, &bar);
+      if (NCT > 0) {
+        for (int rr = 0; rr < rows_here; ++rr)
+          bulk_load(Br + (size_t)rr * ldb, chunk + (size_t)rr * n * kC, rbytes, &bar);
+      } else {
+        bulk_load(Br, chunk, bytes, &bar);
+      }
     }
   } else {
     for (int rr = 0; rr < rows_here; ++rr)
       for (int e = threadIdx.x; e < n; e += blockDim.x)
 #pragma unroll
         for (int c = 0; c < kC; ++c)
-          Br[(rr * n + e) * kC + c] = xl[geom_off(a.g, row0 + rr, e, c)];
+          Br[rr * ldb + e * kC + c] = xl[geom_off(a.g, row0 + rr, e, c)];
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
   // local operator: phase ids of the tile and the (tr, dev) table go to
@@ -200,23 +258,42 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
   } else {
     __syncthreads();
   }
-  for (int rr = 0; rr < R; ++rr)
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      T v[kC];
+  if constexpr (NCT > 0) {
+    // voxel v = (e, rr) with the row fastest (R a compile-time constant)
+    for (int v = threadIdx.x; v < R * n; v += blockDim.x) {
+      const int rr = v % R, e = v / R;
+      T x[kC];
       if (rr < rows_here) {
-#pragma unroll
-        for (int c = 0; c < kC; ++c) v[c] = Br[(rr * n + e) * kC + c];
+        load_voxel<T, kC>(Br + rr * ldb + e * kC, x);
         if constexpr (LOCAL) {
           const int ph = phs[rr * n + e];
-          iso_apply<T>(v, tab[2 * ph], tab[2 * ph + 1], kC == 3 ? 2 : 3);
+          iso_apply<T>(x, tab[2 * ph], tab[2 * ph + 1], kC == 3 ? 2 : 3);
         }
       } else {
 #pragma unroll
-        for (int c = 0; c < kC; ++c) v[c] = T(0);
+        for (int c = 0; c < kC; ++c) x[c] = T(0);
       }
-#pragma unroll
-      for (int c = 0; c < kC; ++c) Ar[e * ldr + rr * kC + c] = v[c];
+      store_voxel<T, kC>(Ar + e * ldr + rr * kC, x);
     }
+  } else {
+    for (int rr = 0; rr < R; ++rr)
+      for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        T v[kC];
+        if (rr < rows_here) {
+#pragma unroll
+          for (int c = 0; c < kC; ++c) v[c] = Br[rr * ldb + e * kC + c];
+          if constexpr (LOCAL) {
+            const int ph = phs[rr * n + e];
+            iso_apply<T>(v, tab[2 * ph], tab[2 * ph + 1], kC == 3 ? 2 : 3);
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < kC; ++c) v[c] = T(0);
+        }
+#pragma unroll
+        for (int c = 0; c < kC; ++c) Ar[e * ldr + rr * kC + c] = v[c];
+      }
+  }
   if (ldr > RC)
     for (int e = threadIdx.x; e < n; e += blockDim.x)
       for (int j = RC; j < ldr; ++j) Ar[e * ldr + j] = T(0);
@@ -301,9 +378,14 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   OT* outchunk = outl + row0 * n * kC;
   const uint32_t ebytes = (uint32_t)(rows_here * n * kC * sizeof(T));
   const uint32_t obytes = (uint32_t)(rows_here * n * kC * sizeof(OT));
+  const uint32_t erow = (uint32_t)(n * kC * sizeof(T)), orow = (uint32_t)(n * kC * sizeof(OT));
+  // side field and output staged [rr][e][c] with rows ldE / ldO reals apart
+  // (padded for the compile-time tiles, one bulk copy per row)
+  const int ldE = n * kC + (NCT > 0 ? row_pad<T, kC>() : 0);
+  const int ldO = n * kC + (NCT > 0 ? row_pad<OT, kC>() : 0);
   const bool bulk_s = aligned16(src) && sbytes % 16 == 0;
-  const bool bulk_e = kSide && a.contig && aligned16(sidechunk) && ebytes % 16 == 0;
-  const bool bulk_o = a.contig && aligned16(outchunk) && obytes % 16 == 0;
+  const bool bulk_e = kSide && a.contig && aligned16(sidechunk) && erow % 16 == 0;
+  const bool bulk_o = a.contig && aligned16(outchunk) && orow % 16 == 0;
   if (threadIdx.x == 0) {
     fail_flag = 0;
     mbar_init(&bar, 1);
@@ -313,7 +395,14 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
   if (threadIdx.x == 0 && (bulk_s || bulk_e)) {
     mbar_arrive_expect_tx(&bar, (bulk_s ? sbytes : 0u) + (bulk_e ? ebytes : 0u));
     if (bulk_s) bulk_load(B, src, sbytes, &bar);
-    if (bulk_e) bulk_load(Eo, sidechunk, ebytes, &bar);
+    if (bulk_e) {
+      if (NCT > 0) {
+        for (int rr = 0; rr < rows_here; ++rr)
+          bulk_load(Eo + (size_t)rr * ldE, sidechunk + (size_t)rr * n * kC, erow, &bar);
+      } else {
+        bulk_load(Eo, sidechunk, ebytes, &bar);
+      }
+    }
   }
   if (!bulk_s) {
     const int cnt = rows_here * m * kC;
@@ -324,7 +413,7 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
       for (int e = threadIdx.x; e < n; e += blockDim.x)
 #pragma unroll
         for (int c = 0; c < kC; ++c)
-          Eo[(rr * n + e) * kC + c] = sidel[geom_off(a.g, row0 + rr, e, c)];
+          Eo[rr * ldE + e * kC + c] = sidel[geom_off(a.g, row0 + rr, e, c)];
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
   if (bulk_s || bulk_e) {
@@ -367,35 +456,69 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
 #pragma unroll
   for (int c = 0; c < kC; ++c)
     Ev[c] = (EPI == kEpiUpdate || EPI == kEpiResid) ? static_cast<T>(a.E[l * kC + c]) : T(0);
-  for (int rr = 0; rr < rows_here; ++rr)
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+  // one voxel: y = tile values, side = staged side field -> output values
+  auto epilogue = [&](const T (&y)[kC], const T (&side)[kC], OT (&out)[kC]) {
 #pragma unroll
-      for (int c = 0; c < kC; ++c) {
-        const T v = Zr[e * ldr + rr * kC + c];
-        const int s = (rr * n + e) * kC + c;
-        if (EPI == kEpiUpdate) {
-          const T old = Eo[s];
-          const T nv = sub_rn(Ev[c], mul_rn(a.scale, v));
-          O[s] = nv;
-          const double d = static_cast<double>(nv) - static_cast<double>(old);
-          acc += d * d;
-        } else if (EPI == kEpiResid) {
-          const T nv = sub_rn(Ev[c], mul_rn(a.scale, v));
-          const double d = static_cast<double>(nv) - static_cast<double>(Eo[s]);
-          O[s] = static_cast<OT>(d);
-          acc += d * d;
-        } else if (EPI == kEpiRhs) {
-          O[s] = static_cast<OT>(sub_rn(Eo[s], mul_rn(a.scale, v)));
-        } else {
-          O[s] = static_cast<OT>(mul_rn(a.scale, v));
-        }
+    for (int c = 0; c < kC; ++c) {
+      if (EPI == kEpiUpdate) {
+        const T nv = sub_rn(Ev[c], mul_rn(a.scale, y[c]));
+        out[c] = nv;
+        const double d = static_cast<double>(nv) - static_cast<double>(side[c]);
+        acc += d * d;
+      } else if (EPI == kEpiResid) {
+        const T nv = sub_rn(Ev[c], mul_rn(a.scale, y[c]));
+        const double d = static_cast<double>(nv) - static_cast<double>(side[c]);
+        out[c] = static_cast<OT>(d);
+        acc += d * d;
+      } else if (EPI == kEpiRhs) {
+        out[c] = static_cast<OT>(sub_rn(side[c], mul_rn(a.scale, y[c])));
+      } else {
+        out[c] = static_cast<OT>(mul_rn(a.scale, y[c]));
       }
     }
+  };
+  if constexpr (NCT > 0) {
+    // voxel v = (e, rr) with the row fastest (R a compile-time constant)
+    for (int v = threadIdx.x; v < R * n; v += blockDim.x) {
+      const int rr = v % R, e = v / R;
+      if (rr >= rows_here) continue;
+      T y[kC], side[kC];
+      OT out[kC];
+      load_voxel<T, kC>(Zr + e * ldr + rr * kC, y);
+      if constexpr (kSide) {
+        load_voxel<T, kC>(Eo + rr * ldE + e * kC, side);
+      } else {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) side[c] = T(0);
+      }
+      epilogue(y, side, out);
+      store_voxel<OT, kC>(O + rr * ldO + e * kC, out);
+    }
+  } else {
+    for (int rr = 0; rr < rows_here; ++rr)
+      for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        T y[kC], side[kC];
+        OT out[kC];
+#pragma unroll
+        for (int c = 0; c < kC; ++c) {
+          y[c] = Zr[e * ldr + rr * kC + c];
+          side[c] = kSide ? Eo[rr * ldE + e * kC + c] : T(0);
+        }
+        epilogue(y, side, out);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) O[rr * ldO + e * kC + c] = out[c];
+      }
+  }
   fence_async_shared();
   __syncthreads();
   if (bulk_o) {
     if (threadIdx.x == 0) {
-      bulk_store(outchunk, O, obytes);
+      if (NCT > 0) {
+        for (int rr = 0; rr < rows_here; ++rr)
+          bulk_store(outchunk + (size_t)rr * n * kC, O + (size_t)rr * ldO, orow);
+      } else {
+        bulk_store(outchunk, O, obytes);
+      }
       bulk_commit();
       bulk_wait_read();
     }
@@ -404,7 +527,7 @@ __global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
       for (int e = threadIdx.x; e < n; e += blockDim.x)
 #pragma unroll
         for (int c = 0; c < kC; ++c)
-          outl[geom_off(a.g, row0 + rr, e, c)] = O[(rr * n + e) * kC + c];
+          outl[geom_off(a.g, row0 + rr, e, c)] = O[rr * ldO + e * kC + c];
   }
   if (EPI == kEpiUpdate || EPI == kEpiResid) {
     const double s = block_sum(acc, red);
@@ -911,22 +1034,29 @@ int tile_threads(int W) {
 // rows per CTA, tile width and shared memory of the contiguous-axis kernels
 // (tiles of (n+2) x W complex, W = ceil(R*C/2); `extra` = the old-strain
 // staging of the update variant)
-size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local) {
+// shared memory of a row kernel: twiddles, two tiles, the side-field rows
+// (solver epilogues; up to 32 bytes of padding between rows) and, with the
+// local operator, the tile's phase ids and the staged phase table.  This is
+// the kernels' exact layout (each region aligned to 16 bytes): three CTAs
+// per SM of the FP64 c2r update kernel at n = 128 fit with 96 bytes to spare.
+size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local, int nphase) {
   const size_t cs = dtype == F64 ? 16 : 8;
-  return n * cs + 2 * (size_t)(n + 2) * w * cs + (update ? (size_t)r * n * C * (cs / 2) : 0) +
-         (local ? (size_t)r * n * 4 + 2 * kTabStage * (cs / 2) + 16 : 0) + 48;
+  const size_t staged = nphase <= kTabStage ? (size_t)nphase : 0;
+  auto a16 = [](size_t v) { return (v + 15) / 16 * 16; };
+  size_t off = a16(n * cs) + (size_t)(n + 2) * w * cs;  // twiddles | A
+  off = a16(off) + (size_t)(n + 2) * w * cs;           // B
+  if (update) off = a16(off) + (size_t)r * n * C * (cs / 2) + (size_t)(r - 1) * 32;
+  if (local) off = a16(off + (size_t)r * n * 4) + 2 * staged * (cs / 2);
+  return off;
 }
 
 bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem,
-                bool local = false) {
+                bool local = false, int nphase = 0) {
   const size_t cs = dtype == F64 ? 16 : 8;
   int r = (24 + C - 1) / C;
   for (;;) {
     const int w = (r * C + 1) / 2;
-    const size_t bytes = n * cs + 2 * (size_t)(n + 2) * w * cs +
-                         (update ? (size_t)r * n * C * (cs / 2) : 0) +
-                         (local ? (size_t)r * n * 4 + 2 * kTabStage * (cs / 2) + 16 : 0) +
-                         48;  // + alignment
+    const size_t bytes = rows_smem(dtype, n, C, r, w, update, local, nphase);
     if (bytes <= kSmemBudget || r == 1) {
       if (bytes > kSmemCap - 4096) return false;
       *R = r;
@@ -1141,7 +1271,9 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   const int n = ax.plan.n;
   if (C != 1 && C != 3 && C != 6) return cudaErrorInvalidValue;
   if (local && C == 1) return cudaErrorInvalidValue;
-  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem, local != nullptr))
+  const int nphase = local ? local->nphase : 0;
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem, local != nullptr,
+                  nphase))
     return cudaErrorInvalidValue;
   a.x = static_cast<const T*>(x);
   a.out = static_cast<cx<T>*>(out);
@@ -1166,7 +1298,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     const int wct = n <= 128 ? 12 : 6;
     const int rct = 2 * wct / C;
     const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, false,
-                                 local != nullptr);
+                                 local != nullptr, nphase);
     if (sct <= kSmemBudget + 24 * 1024) {
       RowsArgs<T> b = a;
       b.R = rct;
@@ -1238,7 +1370,7 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
     const int wct = n <= 128 ? 12 : 6;
     const int rct = 2 * wct / C;
     const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, upd != nullptr,
-                                 false);
+                                 false, 0);
     if (sct <= kSmemBudget + 24 * 1024) {
       RowsArgs<T> b = a;
       b.R = rct;
