@@ -64,6 +64,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
+// hint: bring the 128-byte line holding p into L1 (no effect on results)
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes,
                                           uint64_t* bar) {
   asm volatile(

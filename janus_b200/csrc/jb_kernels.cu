@@ -771,6 +771,15 @@ __global__ void __launch_bounds__(cols_max_threads<NCT, WCT>(), cols_min_blocks<
     if (threadIdx.x == 0 && tn < total) issue_load(tn, in_tile(nb), &bar[nb]);
     use += nb == 0;
     buf = nb;
+    if (MODE == 2 && a.mn != nullptr) {
+      // the tile's M/N slice ([f][c][e], consecutive coefficients adjacent)
+      // heads for L1 while the forward transform runs
+      constexpr int NT = MnSize<DIM>::value;
+      const int nf = (Wc + a.C - 1) / a.C;
+      const char* base = reinterpret_cast<const char*>(a.mn + (size_t)(c0 / a.C) * n * NT);
+      const int lines = (int)(((size_t)nf * n * NT * sizeof(T) + 127) / 128);
+      for (int q = threadIdx.x; q < lines; q += blockDim.x) prefetch_l1(base + (size_t)q * 128);
+    }
     C* Z;
     if constexpr (NCT > 0) {
       if (MODE == 1)
