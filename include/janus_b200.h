@@ -146,7 +146,9 @@ int jb_green_apply_by_freq_device(jb_green *green, int64_t count,
 /* Replaces BlockDiagonalOperator2D/3D built from FourthRankIsotropicTensor
  * local operators (janus/operators.pyx:617-716, 257-408): phase-map form.
  * sph/dev: host arrays of nphase coefficients; phase: device array of
- * n0*n1*(n2) indices, uint8 (index_bytes 1) or int32 (4), copied. */
+ * n0*n1*(n2) indices, uint8 (index_bytes 1) or int32 (4), copied.
+ * index_bytes 0: one (sph, dev) pair per voxel (a stiffness field such as
+ * mu(x)); nphase must equal the voxel count and phase must be NULL. */
 int jb_local_create(int dim, const int64_t *shape, int nphase,
                     const double *sph, const double *dev, const void *phase,
                     int index_bytes, int dtype, jb_local **out);
@@ -155,6 +157,18 @@ int jb_local_destroy(jb_local *local);
  * reference arithmetic; x == y allowed. */
 int jb_local_apply(jb_local *local, const void *x, void *y, int64_t batch,
                    void *stream);
+/* Per-voxel strain / adjoint-strain contraction for the gradient of mean
+ * stresses with respect to a stiffness field (no reference counterpart: the
+ * reference has no derivatives).  eps, zeta: [nload][nvox][s] fields of
+ * `dtype` on the device; out: double[nvox][2] on the device, receiving
+ *   out[v][0] = scale * sum_j tr(zeta_j) tr(eps_j) / dim        (d/d sph)
+ *   out[v][1] = scale * sum_j (zeta_j . eps_j - tr(zeta_j) tr(eps_j) / dim)
+ *                                                             (d/d dev)
+ * i.e. zeta : J : eps and zeta : K : eps with J, K the isotropic projectors
+ * of sph J + dev K (operators.pyx:257-303), in Mandel form. */
+int jb_local_gradient(int dim, int dtype, int64_t nvox, int nload,
+                      const void *eps, const void *zeta, double scale,
+                      double *out, void *stream);
 /* BlockDiagonalLinearOperator2D/3D.c_apply / c_apply_transpose (739-774,
  * 823-861): y[v] = a[v] x[v] (or a[v]^T x[v]); a: T[nvox][osz][isz]. */
 int jb_block_linear_apply(int dtype, int64_t nvox, int osz, int isz,

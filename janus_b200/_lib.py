@@ -60,6 +60,8 @@ _SIGS = {
     "jb_local_apply": ([c_void_p, c_void_p, c_void_p, c_int64, c_void_p], c_int),
     "jb_block_linear_apply": ([c_int, c_int64, c_int, c_int, c_void_p, c_void_p, c_void_p,
                                c_int, c_void_p], c_int),
+    "jb_local_gradient": ([c_int, c_int, c_int64, c_int, c_void_p, c_void_p, c_double,
+                           c_void_p, c_void_p], c_int),
     "jb_solver_create": ([c_void_p, c_void_p, c_int, ctypes.POINTER(c_void_p)], c_int),
     "jb_solver_destroy": ([c_void_p], c_int),
     "jb_solver_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_double, P_double, P_int,

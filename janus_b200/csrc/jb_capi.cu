@@ -750,9 +750,10 @@ int jb_local_create(int dim, const int64_t* shape, int nphase, const double* sph
   if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
   if (dtype != F64 && dtype != F32) return fail(JB_EINVAL, "dtype must be JB_F64 or JB_F32");
   if (nphase < 1) return fail(JB_EINVAL, "nphase must be >= 1");
-  if (index_bytes != 1 && index_bytes != 4) return fail(JB_EINVAL, "index_bytes must be 1 or 4");
+  if (index_bytes != 0 && index_bytes != 1 && index_bytes != 4)
+    return fail(JB_EINVAL, "index_bytes must be 0 (per-voxel field), 1 or 4");
   if (index_bytes == 1 && nphase > 256) return fail(JB_EINVAL, "uint8 phase map allows 256 phases");
-  if (!sph || !dev || !phase) return fail(JB_EINVAL, "NULL argument");
+  if (!sph || !dev || (index_bytes != 0 && !phase)) return fail(JB_EINVAL, "NULL argument");
   jb_local* L = new jb_local();
   L->dim = dim;
   L->dtype = dtype;
@@ -767,6 +768,10 @@ int jb_local_create(int dim, const int64_t* shape, int nphase, const double* sph
     L->n[d] = shape[d];
     L->nvox *= shape[d];
   }
+  if (index_bytes == 0 && (int64_t)nphase != L->nvox) {
+    delete L;
+    return fail(JB_EINVAL, "a per-voxel field needs nphase equal to the voxel count");
+  }
   std::vector<double> tab(2 * (size_t)nphase);
   for (int p = 0; p < nphase; ++p) {
     tab[2 * p] = (sph[p] - dev[p]) / (double)dim;  // operators.pyx:299
@@ -774,7 +779,7 @@ int jb_local_create(int dim, const int64_t* shape, int nphase, const double* sph
   }
   const size_t rs = real_size(dtype);
   int r = dev_alloc(&L->table, tab.size() * rs);
-  if (r == JB_OK) r = dev_alloc(&L->phase, (size_t)L->nvox * index_bytes);
+  if (r == JB_OK && index_bytes != 0) r = dev_alloc(&L->phase, (size_t)L->nvox * index_bytes);
   if (r != JB_OK) {
     if (L->table) cudaFree(L->table);
     delete L;
@@ -787,7 +792,7 @@ int jb_local_create(int dim, const int64_t* shape, int nphase, const double* sph
     std::vector<float> f(tab.begin(), tab.end());
     e = cudaMemcpy(L->table, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
   }
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && index_bytes != 0)
     e = cudaMemcpy(L->phase, phase, (size_t)L->nvox * index_bytes, cudaMemcpyDefault);
   if (e != cudaSuccess) {
     cudaFree(L->table);
@@ -836,6 +841,18 @@ int jb_block_linear_apply(int dtype, int64_t nvox, int osz, int isz, const void*
   return launch_status(jb::launch_block_linear(dtype, nvox, 1, osz, isz, a, x, y, transpose,
                                                as_stream(stream)),
                        "block_linear");
+}
+
+int jb_local_gradient(int dim, int dtype, int64_t nvox, int nload, const void* eps,
+                      const void* zeta, double scale, double* out, void* stream) {
+  if (!eps || !zeta || !out) return fail(JB_EINVAL, "NULL argument");
+  if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
+  if (dtype != F64 && dtype != F32) return fail(JB_EINVAL, "dtype must be JB_F64 or JB_F32");
+  if (nvox < 0 || nload < 1) return fail(JB_EINVAL, "nvox must be >= 0 and nload >= 1");
+  if (nvox == 0) return JB_OK;
+  return launch_status(jb::launch_local_gradient(dtype, dim, nvox, nload, eps, zeta, scale, out,
+                                                 as_stream(stream)),
+                       "local_gradient");
 }
 
 // ---------------------------------------------------------------------------

@@ -68,7 +68,10 @@ __device__ __forceinline__ void iso_apply(T* p, T tr, T dev, int dim) {
   }
 }
 
+// phase id of voxel v: uint8 or int32 map; index_bytes 0 = one table entry
+// per voxel (stiffness fields)
 __device__ __forceinline__ int load_phase(const void* phase, int ib, int64_t v) {
+  if (ib == 0) return static_cast<int>(v);
   return ib == 1 ? static_cast<int>(static_cast<const uint8_t*>(phase)[v])
                  : static_cast<const int32_t*>(phase)[v];
 }
@@ -884,6 +887,37 @@ __global__ void local_sum_kernel(LocalDesc loc, const T* table, int C, int64_t n
   }
 }
 
+// out[v] = scale * sum_j (tr z_j tr e_j / dim, z_j . e_j - tr z_j tr e_j / dim):
+// the isotropic-projector contractions of strain and adjoint strain
+template <typename T>
+__global__ void local_gradient_kernel(int dim, int64_t nvox, int L, const T* __restrict__ eps,
+                                      const T* __restrict__ zeta, double scale,
+                                      double* __restrict__ out) {
+  const int C = dim == 2 ? 3 : 6;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    double sj = 0.0, sk = 0.0;
+    for (int l = 0; l < L; ++l) {
+      const T* e = eps + ((int64_t)l * nvox + v) * C;
+      const T* z = zeta + ((int64_t)l * nvox + v) * C;
+      double tre = 0.0, trz = 0.0, dot = 0.0;
+      for (int c = 0; c < C; ++c) {
+        const double ec = static_cast<double>(e[c]), zc = static_cast<double>(z[c]);
+        dot += zc * ec;
+        if (c < dim) {
+          tre += ec;
+          trz += zc;
+        }
+      }
+      const double j = tre * trz / dim;
+      sj += j;
+      sk += dot - j;
+    }
+    out[2 * v] = scale * sj;
+    out[2 * v + 1] = scale * sk;
+  }
+}
+
 template <typename T>
 __global__ void block_linear_kernel(int64_t nvox, int L, int osz, int isz, const T* a,
                                     const T* x, T* y, int transpose) {
@@ -1596,6 +1630,21 @@ cudaError_t launch_local_sum(int dtype, const LocalDesc& loc, int C, int L, int6
     local_sum_kernel<float><<<grid, kThreads, 0, st>>>(
         loc, static_cast<const float*>(loc.table), C, nvox, static_cast<const float*>(eps),
         partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_local_gradient(int dtype, int dim, int64_t nvox, int L, const void* eps,
+                                  const void* zeta, double scale, double* out,
+                                  cudaStream_t st) {
+  const int grid = grid_for(nvox);
+  if (dtype == F64)
+    local_gradient_kernel<double><<<grid, kThreads, 0, st>>>(
+        dim, nvox, L, static_cast<const double*>(eps), static_cast<const double*>(zeta), scale,
+        out);
+  else
+    local_gradient_kernel<float><<<grid, kThreads, 0, st>>>(
+        dim, nvox, L, static_cast<const float*>(eps), static_cast<const float*>(zeta), scale,
+        out);
   return cudaGetLastError();
 }
 

@@ -116,6 +116,11 @@ cudaError_t launch_reduce_rows(const double* partials, int L, int nb, double* ou
 cudaError_t launch_local_sum(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
                              const void* eps, double* partials, int* nblocks_out,
                              cudaStream_t st);
+// per-voxel strain / adjoint-strain contractions (gradient of mean stresses
+// with respect to the (sph, dev) field): out double[nvox][2]
+cudaError_t launch_local_gradient(int dtype, int dim, int64_t nvox, int L, const void* eps,
+                                  const void* zeta, double scale, double* out,
+                                  cudaStream_t st);
 cudaError_t launch_reduce_cols(const double* partials, int L, int C, int nb, double* out,
                                double factor, cudaStream_t st);
 

@@ -135,7 +135,7 @@ def gaussian_field(n, dim=3, corr_len=8.0, std=1.5, seed=0):
     k2 = sum(kk * kk for kk in K)
     # amplitude = sqrt of the spectral density of the SE covariance
     amp = np.exp(-0.25 * corr_len ** 2 * k2)
-    g = np.fft.irfftn(np.fft.rfftn(w) * amp, s=shape)
+    g = np.fft.irfftn(np.fft.rfftn(w) * amp, s=shape, axes=tuple(range(dim)))
     g -= g.mean()
     g *= std / g.std()
     return g

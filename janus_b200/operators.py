@@ -259,12 +259,19 @@ class AbstractStructuredOperator3D(_AbstractStructuredOperator):
 
 class LocalPhaseOperator:
     """Device form of (C - C0):eps on a phase map: the native handle plus
-    the phase map, for the solver and the block-diagonal operators."""
+    the phase map, for the solver and the block-diagonal operators.
+
+    ``phase=None`` makes it a stiffness field: ``sph`` and ``dev`` then hold
+    one coefficient per voxel (C order over the grid), as for mu(x)."""
 
     def __init__(self, dim, shape, phase, sph, dev, dtype=torch.float64):
         self.dim = int(dim)
         self.shape = tuple(int(v) for v in shape)
         self.dtype = dtype
+        if A.is_tensor(sph):
+            sph = sph.detach().cpu().numpy()
+        if A.is_tensor(dev):
+            dev = dev.detach().cpu().numpy()
         sph = np.ascontiguousarray(np.asarray(sph, dtype=np.float64).ravel())
         dev = np.ascontiguousarray(np.asarray(dev, dtype=np.float64).ravel())
         if sph.shape != dev.shape:
@@ -272,6 +279,18 @@ class LocalPhaseOperator:
         self.nphase = int(sph.shape[0])
         self.sph = sph
         self.dev = dev
+        if phase is None:
+            nvox = int(np.prod(self.shape))
+            if self.nphase != nvox:
+                raise ValueError("a stiffness field needs one (sph, dev) pair per voxel "
+                                 "({} given for {} voxels)".format(self.nphase, nvox))
+            self.phase = None
+            self._handle = ctypes.c_void_p()
+            _lib.check(_lib.lib().jb_local_create(
+                self.dim, _lib.i64_array(self.shape), self.nphase, sph.ctypes.data_as(_P),
+                dev.ctypes.data_as(_P), None, 0, A.jb_dtype(dtype),
+                ctypes.byref(self._handle)))
+            return
         index_bytes = 1 if self.nphase <= 256 else 4
         if A.is_tensor(phase):
             ph = phase.to(A.device())

@@ -373,3 +373,48 @@ def delta_c(mat_g, mat_nu, g0, nu0, dim):
     k = bulk_modulus(mat_g, mat_nu, dim)
     k0 = bulk_modulus(g0, nu0, dim)
     return dim * (k - k0), 2 * (mat_g - g0)
+
+
+# --------------------------------------------------------------------------
+# gradients with respect to a stiffness field (no reference counterpart: the
+# reference has no derivatives; these restate the adjoint of its basic
+# scheme, square_basic.py:83-97, and check it by differencing that scheme)
+# --------------------------------------------------------------------------
+
+def local_gradient(eps, zeta, dim, scale):
+    """Per voxel, scale * sum over load cases of the contractions of the
+    adjoint strain zeta and the strain eps with the isotropic projectors
+    J and K of operators.pyx:257-303 (Mandel form):
+        out[..., 0] = scale * sum_j tr(zeta_j) tr(eps_j) / dim
+        out[..., 1] = scale * sum_j (zeta_j . eps_j - tr(zeta_j) tr(eps_j) / dim)
+    eps, zeta: (nload, *grid, s)."""
+    eps = np.asarray(eps, dtype=np.float64)
+    zeta = np.asarray(zeta, dtype=np.float64)
+    tre = eps[..., :dim].sum(axis=-1)
+    trz = zeta[..., :dim].sum(axis=-1)
+    j = tre * trz / dim
+    k = (zeta * eps).sum(axis=-1) - j
+    return scale * np.stack([j.sum(axis=0), k.sum(axis=0)], axis=-1)
+
+
+def field_tables(mu, nu, g0, nu0):
+    """(phase map, sph, dev) of C - C0 for a per-voxel shear modulus mu at a
+    uniform Poisson ratio nu: one table entry per voxel (square_basic.py:26-29
+    applied voxel by voxel)."""
+    mu = np.asarray(mu, dtype=np.float64)
+    dim = mu.ndim
+    phase = np.arange(mu.size).reshape(mu.shape)
+    k = bulk_modulus(mu.ravel(), nu, dim)
+    k0 = bulk_modulus(g0, nu0, dim)
+    return phase, dim * (k - k0), 2 * (mu.ravel() - g0)
+
+
+def field_mean_stress(mu, nu, g0, nu0, avg_eps, num_iter, tol, variant="truncated"):
+    """Mean stress C0:E + <tau> of a stiffness field under one load case,
+    by the oracle basic scheme."""
+    phase, sph, dev = field_tables(mu, nu, g0, nu0)
+    dim = np.asarray(mu).ndim
+    _, res, tau = basic_scheme(phase, sph, dev, g0, nu0, avg_eps, num_iter,
+                               variant=variant, tol=tol)
+    k0 = bulk_modulus(g0, nu0, dim)
+    return isotropic_apply(np.asarray(avg_eps, dtype=np.float64), dim * k0, 2 * g0, dim) + tau

@@ -147,3 +147,41 @@ def test_oracle_basic_scheme_matches_reference_build(variant, shape):
         eps, new = new, eps
     np.testing.assert_allclose(eps_o, eps, rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(res_o, res, rtol=1e-10)
+
+
+def _field_2d(n, seed, std=0.6):
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((n, n))
+    # smooth a little so that neighbouring voxels correlate
+    g = 0.5 * g + 0.125 * (np.roll(g, 1, 0) + np.roll(g, -1, 0) + np.roll(g, 1, 1) +
+                           np.roll(g, -1, 1))
+    g = (g - g.mean()) * (std / g.std())
+    return np.exp(g)
+
+
+@pytest.mark.parametrize("cot", [(0.0, 0.0, 1.0), (0.3, -0.2, 1.0)])
+def test_oracle_adjoint_gradient_matches_differences(cot):
+    """The adjoint formula dJ/dmu(x) = (1/N) zeta.dC/dmu.eps, with zeta the
+    basic-scheme solution for the cotangent as macroscopic strain, against
+    central differences of the oracle's basic scheme (stiffness field, 2D)."""
+    n, nu = 12, 0.3
+    mu = _field_2d(n, 5)
+    g0 = 0.5 * (mu.min() + mu.max())
+    E = np.array([0.0, 0.0, 1.0])
+    G = np.asarray(cot)
+    tol, its = 1e-15, 3000
+    phase, sph, dev = O.field_tables(mu, nu, g0, nu)
+    eps, _, _ = O.basic_scheme(phase, sph, dev, g0, nu, E, its, tol=tol)
+    zeta, _, _ = O.basic_scheme(phase, sph, dev, g0, nu, G, its, tol=tol)
+    out = O.local_gradient(eps[None], zeta[None], 2, 1.0 / mu.size)
+    grad = out[..., 0] * 2 * O.bulk_modulus(1.0, nu, 2) + out[..., 1] * 2.0
+    rng = np.random.default_rng(1)
+    for v in rng.choice(mu.size, 4, replace=False):
+        h = 1e-4 * mu.flat[v]
+        vals = []
+        for sgn in (1, -1):
+            m = mu.copy()
+            m.flat[v] += sgn * h
+            vals.append(G @ O.field_mean_stress(m, nu, g0, nu, E, its, tol))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - grad.flat[v]) <= 1e-6 * abs(grad).max(), (v, fd, grad.flat[v])
