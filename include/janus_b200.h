@@ -223,6 +223,28 @@ int jb_mixed_run(jb_mixed *solver, const double *E, void *eps, int init,
                  int *outer_out, int *fp32_iters_out, double *mean_tau,
                  void *stream);
 
+/* Batched mixed-precision solves (no reference counterpart): `count`
+ * problems, each a jb_mixed solver of its own grid (sizes may differ) and
+ * load cases.  jb_batch_run evaluates every problem's first FP64 residual,
+ * then launches one CUDA graph per outer step that holds, for every problem
+ * still iterating, the FP32 correction sweeps and the next FP64 residual;
+ * the problems run on `branches` parallel streams inside the graph (largest
+ * first onto the least loaded).  The graph is captured again only when a
+ * problem leaves the iteration (converged or at max_outer).  Arrays are
+ * concatenated in problem order: E host double[L_p][s_p]; eps device
+ * pointers (FP64 fields [L_p][grid_p][s_p]); residuals host
+ * double[max_outer][L_p] per problem (may be NULL); outer_out /
+ * fp32_iters_out int[count]; mean_tau host double[L_p][s_p] (may be NULL);
+ * graph_launches_out: graph launches made.  The handles are borrowed. */
+typedef struct jb_batch_s jb_batch;
+int jb_batch_create(int count, jb_mixed *const *problems, int branches,
+                    jb_batch **out);
+int jb_batch_destroy(jb_batch *batch);
+int jb_batch_run(jb_batch *batch, const double *E, void *const *eps, int init,
+                 int max_outer, int inner, double tol, double *residuals,
+                 int *outer_out, int *fp32_iters_out, double *mean_tau,
+                 int *graph_launches_out, void *stream);
+
 /* Benchmark support: record CUDA events around every pass of the next
  * `max_steps` calls of jb_solver_step (on their stream). */
 int jb_solver_timing_begin(jb_solver *solver, int max_steps);

@@ -62,6 +62,11 @@ _SIGS = {
                                c_int, c_void_p], c_int),
     "jb_local_gradient": ([c_int, c_int, c_int64, c_int, c_void_p, c_void_p, c_double,
                            c_void_p, c_void_p], c_int),
+    "jb_batch_create": ([c_int, ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)],
+                        c_int),
+    "jb_batch_destroy": ([c_void_p], c_int),
+    "jb_batch_run": ([c_void_p, P_double, ctypes.POINTER(c_void_p), c_int, c_int, c_int,
+                      c_double, P_double, P_int, P_int, P_double, P_int, c_void_p], c_int),
     "jb_solver_create": ([c_void_p, c_void_p, c_int, ctypes.POINTER(c_void_p)], c_int),
     "jb_solver_destroy": ([c_void_p], c_int),
     "jb_solver_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_double, P_double, P_int,

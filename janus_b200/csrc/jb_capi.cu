@@ -323,6 +323,22 @@ int upload_table(jb_green* g, int dtype, const std::vector<double>& v, void** ou
 
 // spectral passes shared by jb_green_apply and the solver
 // x: real fields (or eps with local), spec: complex scratch, y: output
+// the operator's M/N tensors at every half-spectrum coefficient, built once
+// on first use (or ahead of a graph capture)
+int green_prepare(jb_green* g, cudaStream_t st) {
+  if (!g->use_table || g->gt.mn) return JB_OK;
+  const int dim = g->dim;
+  const int64_t n0 = g->n[0], n1 = g->n[1];
+  const int64_t m = (dim == 2 ? g->n[1] : g->n[2]) / 2 + 1;
+  const int NT = dim == 3 ? 21 : 8;
+  const size_t bytes = (size_t)n0 * (dim == 3 ? n1 * m : m) * NT * real_size(g->dtype);
+  JB_TRY(ensure_buf(g->mnbuf, bytes));
+  JB_TRY(launch_status(jb::launch_green_table(g->dtype, dim, g->gt, n0, n1, m, g->mnbuf.p, st),
+                       "green_table"));
+  g->gt.mn = g->mnbuf.p;
+  return JB_OK;
+}
+
 int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
                  const jb::LocalDesc* local, const jb::UpdateDesc* upd, int* nb_rows,
                  cudaStream_t st, PassRecorder* rec = nullptr) {
@@ -362,15 +378,7 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
     rec->mark(st);
   }
   const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
-  if (g->use_table && !g->gt.mn) {
-    // the operator's M/N tensors at every half-spectrum coefficient, once
-    const int NT = dim == 3 ? 21 : 8;
-    const size_t bytes = (size_t)n0 * (dim == 3 ? n1 * m : m) * NT * real_size(g->dtype);
-    JB_TRY(ensure_buf(g->mnbuf, bytes));
-    JB_TRY(launch_status(jb::launch_green_table(g->dtype, dim, g->gt, n0, n1, m, g->mnbuf.p, st),
-                         "green_table"));
-    g->gt.mn = g->mnbuf.p;
-  }
+  JB_TRY(green_prepare(g, st));
   JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
                                        &g->gt, n1, m, st),
                        "cols_green_axis0"));
@@ -1249,18 +1257,14 @@ extern "C" int jb_mixed_destroy(jb_mixed* M) {
   return JB_OK;
 }
 
-extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, int max_outer,
-                            int inner, double tol, double* residuals, int* outer_out,
-                            int* fp32_iters_out, double* mean_tau, void* stream) {
-  if (!M || !E || !eps) return fail(JB_EINVAL, "NULL argument");
-  if (max_outer < 0) return fail(JB_EINVAL, "max_outer must be >= 0");
-  if (inner < 1) return fail(JB_EINVAL, "inner must be >= 1");
-  cudaStream_t st = as_stream(stream);
+namespace {
+
+// load E (host, L x C) for a mixed solver: device copy, residual
+// normalisation 1/(sqrt(N) |E_l|), and eps = E when init
+int mixed_set_load(jb_mixed* M, const double* E, void* eps, int init, cudaStream_t st) {
   const int dim = M->g64->dim;
   const int C = dim == 2 ? 3 : 6;
   const int L = M->L;
-  const int64_t nvox = M->l64->nvox;
-  const int64_t nel = (int64_t)L * nvox * C;
   double N = 1;
   for (int d = 0; d < dim; ++d) N *= (double)M->g64->n[d];
   M->norm.resize(L);
@@ -1274,27 +1278,82 @@ extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, i
   JB_CUDA(cudaMemcpyAsync(M->normd.p, M->norm.data(), sizeof(double) * L,
                           cudaMemcpyHostToDevice, st));
   if (init)
-    JB_TRY(launch_status(jb::launch_fill_macro(F64, C, L, nvox,
+    JB_TRY(launch_status(jb::launch_fill_macro(F64, C, L, M->l64->nvox,
                                                static_cast<const double*>(M->E.p), eps, st),
                          "fill"));
-  jb::LocalDesc loc64 = local_desc(M->l64), loc32 = local_desc(M->l32);
+  return JB_OK;
+}
+
+// FP64 residual pass: r32 = E - eps - Gamma0[(C - C0):eps] (FP32), its
+// normalised norms into res_out (device double[L])
+int mixed_residual(jb_mixed* M, void* eps, double* res_out, cudaStream_t st) {
+  jb::LocalDesc loc64 = local_desc(M->l64);
+  jb::UpdateDesc u;
+  u.mode = 2;
+  u.eps = eps;
+  u.E = static_cast<const double*>(M->E.p);
+  u.partials = static_cast<double*>(M->partials.p);
+  u.rout = static_cast<float*>(M->r32.p);
+  int nb = 0;
+  JB_TRY(green_passes(M->g64, eps, eps, M->L, M->spec.p, &loc64, &u, &nb, st));
+  return launch_status(jb::launch_reduce_rows(static_cast<const double*>(M->partials.p), M->L,
+                                              nb, res_out, 1.0,
+                                              static_cast<const double*>(M->normd.p), 1, st),
+                       "reduce");
+}
+
+// correction: d = r, inner - 1 FP32 sweeps d <- r - Gamma0[(C - C0):d],
+// eps += d
+int mixed_correct(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
+  const int C = M->g64->dim == 2 ? 3 : 6;
+  const int64_t nel = (int64_t)M->L * M->l64->nvox * C;
+  jb::LocalDesc loc32 = local_desc(M->l32);
   float* r32 = static_cast<float*>(M->r32.p);
   float* d32 = static_cast<float*>(M->d32.p);
+  JB_CUDA(cudaMemcpyAsync(d32, r32, sizeof(float) * nel, cudaMemcpyDeviceToDevice, st));
+  for (int j = 1; j < inner; ++j) {
+    jb::UpdateDesc v;
+    v.mode = 3;
+    v.eps = d32;
+    v.rhs = r32;
+    JB_TRY(green_passes(M->g32, d32, d32, M->L, M->spec.p, &loc32, &v, nullptr, st));
+  }
+  return launch_status(jb::launch_axpy_f32_to_f64(nel, d32, static_cast<double*>(eps), st),
+                       "axpy");
+}
+
+// mean of (C - C0):eps per load case and component into host mean_tau
+int mixed_mean(jb_mixed* M, const void* eps, double* mean_tau, cudaStream_t st) {
+  const int C = M->g64->dim == 2 ? 3 : 6;
+  jb::LocalDesc loc64 = local_desc(M->l64);
+  int nb = 0;
+  JB_TRY(launch_status(jb::launch_local_sum(F64, loc64, C, M->L, M->l64->nvox, eps,
+                                            static_cast<double*>(M->partials.p), &nb, st),
+                       "local_sum"));
+  JB_TRY(launch_status(jb::launch_reduce_cols(static_cast<const double*>(M->partials.p), M->L,
+                                              C, nb, static_cast<double*>(M->mean.p),
+                                              1.0 / (double)M->l64->nvox, st),
+                       "reduce"));
+  JB_CUDA(cudaMemcpyAsync(mean_tau, M->mean.p, sizeof(double) * M->L * C,
+                          cudaMemcpyDeviceToHost, st));
+  return JB_OK;
+}
+
+}  // namespace
+
+extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, int max_outer,
+                            int inner, double tol, double* residuals, int* outer_out,
+                            int* fp32_iters_out, double* mean_tau, void* stream) {
+  if (!M || !E || !eps) return fail(JB_EINVAL, "NULL argument");
+  if (max_outer < 0) return fail(JB_EINVAL, "max_outer must be >= 0");
+  if (inner < 1) return fail(JB_EINVAL, "inner must be >= 1");
+  cudaStream_t st = as_stream(stream);
+  const int L = M->L;
+  JB_TRY(mixed_set_load(M, E, eps, init, st));
   std::vector<double> r(L);
   int outer = 0, fp32 = 0;
   for (; outer < max_outer; ++outer) {
-    jb::UpdateDesc u;
-    u.mode = 2;
-    u.eps = eps;
-    u.E = static_cast<const double*>(M->E.p);
-    u.partials = static_cast<double*>(M->partials.p);
-    u.rout = r32;
-    int nb = 0;
-    JB_TRY(green_passes(M->g64, eps, eps, L, M->spec.p, &loc64, &u, &nb, st));
-    JB_TRY(launch_status(jb::launch_reduce_rows(static_cast<const double*>(M->partials.p), L,
-                                                nb, static_cast<double*>(M->res.p), 1.0,
-                                                static_cast<const double*>(M->normd.p), 1, st),
-                         "reduce"));
+    JB_TRY(mixed_residual(M, eps, static_cast<double*>(M->res.p), st));
     JB_CUDA(cudaMemcpyAsync(r.data(), M->res.p, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
     JB_CUDA(cudaStreamSynchronize(st));
     bool done = true;
@@ -1306,33 +1365,220 @@ extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, i
       ++outer;
       break;
     }
-    // correction: d = r, then inner - 1 FP32 sweeps of d <- r - Gamma0[(C-C0):d]
-    JB_CUDA(cudaMemcpyAsync(d32, r32, sizeof(float) * nel, cudaMemcpyDeviceToDevice, st));
-    for (int j = 1; j < inner; ++j) {
-      jb::UpdateDesc v;
-      v.mode = 3;
-      v.eps = d32;
-      v.rhs = r32;
-      JB_TRY(green_passes(M->g32, d32, d32, L, M->spec.p, &loc32, &v, nullptr, st));
-      ++fp32;
-    }
-    JB_TRY(launch_status(jb::launch_axpy_f32_to_f64(nel, d32, static_cast<double*>(eps), st),
-                         "axpy"));
+    JB_TRY(mixed_correct(M, eps, inner, st));
+    fp32 += inner - 1;
   }
   if (outer_out) *outer_out = outer;
   if (fp32_iters_out) *fp32_iters_out = fp32;
-  if (mean_tau) {
-    int nb = 0;
-    JB_TRY(launch_status(jb::launch_local_sum(F64, loc64, C, L, nvox, eps,
-                                              static_cast<double*>(M->partials.p), &nb, st),
-                         "local_sum"));
-    JB_TRY(launch_status(jb::launch_reduce_cols(static_cast<const double*>(M->partials.p), L, C,
-                                                nb, static_cast<double*>(M->mean.p),
-                                                1.0 / (double)nvox, st),
-                         "reduce"));
-    JB_CUDA(cudaMemcpyAsync(mean_tau, M->mean.p, sizeof(double) * L * C, cudaMemcpyDeviceToHost,
-                            st));
+  if (mean_tau) JB_TRY(mixed_mean(M, eps, mean_tau, st));
+  JB_CUDA(cudaStreamSynchronize(st));
+  return JB_OK;
+}
+
+// ===========================================================================
+// batched mixed-precision solves: many problems (uneven grids), one CUDA
+// graph launch per outer step
+// ===========================================================================
+
+struct jb_batch_s {
+  std::vector<jb_mixed*> prob;
+  std::vector<int> branch;             // branch stream of each problem
+  std::vector<size_t> res_off;         // offset of each problem's residuals in res_all
+  int nbranch = 1;
+  std::vector<cudaStream_t> streams;   // capture origin + branches
+  std::vector<cudaEvent_t> events;     // fork / join
+  DeviceBuf res_all;
+  size_t nres = 0;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<char> captured;          // active set of the instantiated graph
+};
+
+extern "C" int jb_batch_destroy(jb_batch* B) {
+  if (!B) return JB_OK;
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  for (cudaStream_t s : B->streams) cudaStreamDestroy(s);
+  for (cudaEvent_t e : B->events) cudaEventDestroy(e);
+  if (B->res_all.p) cudaFree(B->res_all.p);
+  delete B;
+  return JB_OK;
+}
+
+extern "C" int jb_batch_create(int count, jb_mixed* const* problems, int branches,
+                               jb_batch** out) {
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  if (count < 1 || !problems) return fail(JB_EINVAL, "a batch needs at least one problem");
+  if (branches < 1 || branches > 64) return fail(JB_EINVAL, "branches must be in [1, 64]");
+  jb_batch* B = new jb_batch();
+  B->prob.assign(problems, problems + count);
+  for (jb_mixed* M : B->prob)
+    if (!M) {
+      delete B;
+      return fail(JB_EINVAL, "NULL problem");
+    }
+  // longest-processing-time assignment of problems to branches by work
+  B->nbranch = std::min(branches, count);
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  auto work = [&](int i) { return (double)B->prob[i]->L * (double)B->prob[i]->l64->nvox; };
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  std::vector<double> load(B->nbranch, 0.0);
+  B->branch.assign(count, 0);
+  for (int i : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    B->branch[i] = k;
+    load[k] += work(i);
   }
+  B->res_off.resize(count);
+  for (int i = 0; i < count; ++i) {
+    B->res_off[i] = B->nres;
+    B->nres += B->prob[i]->L;
+  }
+  int r = ensure_buf(B->res_all, sizeof(double) * B->nres);
+  B->streams.assign(B->nbranch + 1, nullptr);
+  B->events.assign(2 * B->nbranch + 1, nullptr);
+  for (auto& s : B->streams)
+    if (r == JB_OK && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+      r = fail(JB_ECUDA, "jb_batch_create: cudaStreamCreate failed");
+  for (auto& e : B->events)
+    if (r == JB_OK && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+      r = fail(JB_ECUDA, "jb_batch_create: cudaEventCreate failed");
+  if (r != JB_OK) {
+    cudaGetLastError();
+    jb_batch_destroy(B);
+    return r;
+  }
+  *out = B;
+  return JB_OK;
+}
+
+namespace {
+
+// capture one outer step (correction, then residual) of the active problems:
+// the origin stream forks to the branch streams and joins them again
+int batch_capture(jb_batch* B, const std::vector<char>& active, void* const* eps, int inner) {
+  cudaStream_t origin = B->streams[0];
+  double* res = static_cast<double*>(B->res_all.p);
+  JB_CUDA(cudaStreamBeginCapture(origin, cudaStreamCaptureModeRelaxed));
+  int r = JB_OK;
+  cudaError_t e = cudaEventRecord(B->events[0], origin);
+  for (int k = 0; k < B->nbranch && e == cudaSuccess; ++k)
+    e = cudaStreamWaitEvent(B->streams[k + 1], B->events[0], 0);
+  for (size_t i = 0; i < B->prob.size() && r == JB_OK && e == cudaSuccess; ++i) {
+    if (!active[i]) continue;
+    cudaStream_t st = B->streams[B->branch[i] + 1];
+    r = mixed_correct(B->prob[i], eps[i], inner, st);
+    if (r == JB_OK) r = mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st);
+  }
+  for (int k = 0; k < B->nbranch && e == cudaSuccess; ++k) {
+    e = cudaEventRecord(B->events[k + 1], B->streams[k + 1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(origin, B->events[k + 1], 0);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(origin, &graph);
+  if (r != JB_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return r;
+  }
+  if (e != cudaSuccess || ee != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return fail(JB_ECUDA, std::string("jb_batch_run: capture: ") +
+                              cudaGetErrorString(e != cudaSuccess ? e : ee));
+  }
+  if (B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  e = cudaGraphInstantiate(&B->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    B->exec = nullptr;
+    return fail(JB_ECUDA, std::string("jb_batch_run: instantiate: ") + cudaGetErrorString(e));
+  }
+  B->captured = active;
+  return JB_OK;
+}
+
+}  // namespace
+
+extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int init,
+                            int max_outer, int inner, double tol, double* residuals,
+                            int* outer_out, int* fp32_iters_out, double* mean_tau,
+                            int* graph_launches_out, void* stream) {
+  if (!B || !E || !eps) return fail(JB_EINVAL, "NULL argument");
+  if (max_outer < 1) return fail(JB_EINVAL, "max_outer must be >= 1");
+  if (inner < 1) return fail(JB_EINVAL, "inner must be >= 1");
+  const size_t P = B->prob.size();
+  for (size_t i = 0; i < P; ++i)
+    if (!eps[i]) return fail(JB_EINVAL, "NULL strain field");
+  cudaStream_t st = as_stream(stream);
+  cudaStream_t origin = B->streams[0];
+  double* res = static_cast<double*>(B->res_all.p);
+  // loads, then the first residual of every problem (eagerly: this also
+  // builds each operator's lazily created tables before any capture)
+  size_t eoff = 0;
+  for (size_t i = 0; i < P; ++i) {
+    jb_mixed* M = B->prob[i];
+    const int C = M->g64->dim == 2 ? 3 : 6;
+    JB_TRY(mixed_set_load(M, E + eoff, eps[i], init, st));
+    eoff += (size_t)M->L * C;
+  }
+  for (size_t i = 0; i < P; ++i) {
+    JB_TRY(green_prepare(B->prob[i]->g32, st));  // nothing lazily built inside a capture
+    JB_TRY(mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st));
+  }
+  std::vector<double> rh(B->nres);
+  std::vector<int> outer(P, 1);
+  std::vector<char> active(P, 1);
+  size_t roff = 0;
+  std::vector<size_t> hist_off(P);
+  for (size_t i = 0; i < P; ++i) {
+    hist_off[i] = roff;
+    roff += (size_t)max_outer * B->prob[i]->L;
+  }
+  int launches = 0;
+  for (int step = 0;; ++step) {
+    JB_CUDA(cudaMemcpyAsync(rh.data(), res, sizeof(double) * B->nres, cudaMemcpyDeviceToHost,
+                            step == 0 ? st : origin));
+    JB_CUDA(cudaStreamSynchronize(step == 0 ? st : origin));
+    bool any = false;
+    for (size_t i = 0; i < P; ++i) {
+      if (!active[i]) continue;
+      const int L = B->prob[i]->L;
+      bool done = true;
+      for (int l = 0; l < L; ++l) {
+        const double v = rh[B->res_off[i] + l];
+        if (residuals) residuals[hist_off[i] + (size_t)(outer[i] - 1) * L + l] = v;
+        if (!(v <= tol)) done = false;
+      }
+      if (done || outer[i] >= max_outer) active[i] = 0;
+      any = any || active[i];
+    }
+    if (!any) break;
+    if (!B->exec || B->captured != active) JB_TRY(batch_capture(B, active, eps, inner));
+    if (step == 0) {
+      // order the graph after the eager work on the caller's stream
+      JB_CUDA(cudaEventRecord(B->events[B->nbranch + 1], st));
+      JB_CUDA(cudaStreamWaitEvent(origin, B->events[B->nbranch + 1], 0));
+    }
+    JB_CUDA(cudaGraphLaunch(B->exec, origin));
+    ++launches;
+    for (size_t i = 0; i < P; ++i)
+      if (active[i]) ++outer[i];
+  }
+  // the caller's stream continues after the graph work
+  JB_CUDA(cudaEventRecord(B->events[0], origin));
+  JB_CUDA(cudaStreamWaitEvent(st, B->events[0], 0));
+  eoff = 0;
+  for (size_t i = 0; i < P; ++i) {
+    jb_mixed* M = B->prob[i];
+    const int C = M->g64->dim == 2 ? 3 : 6;
+    if (outer_out) outer_out[i] = outer[i];
+    if (fp32_iters_out) fp32_iters_out[i] = (outer[i] - 1) * (inner - 1);
+    if (mean_tau) JB_TRY(mixed_mean(M, eps[i], mean_tau + eoff, st));
+    eoff += (size_t)M->L * C;
+  }
+  if (graph_launches_out) *graph_launches_out = launches;
   JB_CUDA(cudaStreamSynchronize(st));
   return JB_OK;
 }

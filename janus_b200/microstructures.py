@@ -139,3 +139,36 @@ def gaussian_field(n, dim=3, corr_len=8.0, std=1.5, seed=0):
     g -= g.mean()
     g *= std / g.std()
     return g
+
+
+BATCH_2D_SIZES = (64, 96, 128, 192, 256, 384, 512, 768, 1024)
+
+
+def batch_2d_problems(count=64, seed=0, sizes=BATCH_2D_SIZES):
+    """Seeded batch of two-phase 2D cells of uneven sizes: each draws its
+    grid n from ``sizes``, 2-20 ellipses (semi-axes U[4, n/8], uniform
+    orientation and centres, periodic wrap) of one inclusion phase, an
+    inclusion/matrix shear contrast log-uniform in [10, 1000] (matrix
+    mu = 1), Poisson ratios U[0.15, 0.4] per phase, and the reference medium
+    at the midpoints of the phases' shear and (plane-strain) bulk moduli:
+    mu0 = (mu_min + mu_max)/2, k0 = (k_min + k_max)/2, nu0 = (k0 - mu0)/(2 k0)
+    (isotropic.pyx:32-46).  The basic scheme converges only if k0 exceeds
+    k_max/2; nu0 = the matrix's nu can violate that when the inclusion's nu
+    is the larger one.  Returns a list of dicts with keys n, phase (uint8 0/1
+    map), mu, nu (per phase), mu0, nu0."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice(sizes))
+        k = int(rng.integers(2, 21))
+        sub = int(rng.integers(0, 2 ** 31 - 1))
+        phase = (ellipses(n, k, seed=sub) > 0).astype(np.uint8)
+        contrast = float(np.exp(rng.uniform(np.log(10.0), np.log(1000.0))))
+        nu = rng.uniform(0.15, 0.4, size=2)
+        mu = np.array([1.0, contrast])
+        k = mu / (1.0 - 2.0 * nu)
+        mu0 = 0.5 * (mu.min() + mu.max())
+        k0 = 0.5 * (k.min() + k.max())
+        out.append({"n": n, "phase": phase, "mu": mu, "nu": nu, "mu0": mu0,
+                    "nu0": float((k0 - mu0) / (2.0 * k0))})
+    return out
