@@ -1391,6 +1391,8 @@ struct jb_batch_s {
   size_t nres = 0;
   cudaGraphExec_t exec = nullptr;
   std::vector<char> captured;          // active set of the instantiated graph
+  std::vector<void*> captured_eps;     // the strain fields its kernels address
+  int captured_inner = 0;
 };
 
 extern "C" int jb_batch_destroy(jb_batch* B) {
@@ -1496,6 +1498,8 @@ int batch_capture(jb_batch* B, const std::vector<char>& active, void* const* eps
     return fail(JB_ECUDA, std::string("jb_batch_run: instantiate: ") + cudaGetErrorString(e));
   }
   B->captured = active;
+  B->captured_eps.assign(eps, eps + B->prob.size());
+  B->captured_inner = inner;
   return JB_OK;
 }
 
@@ -1555,7 +1559,11 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
       any = any || active[i];
     }
     if (!any) break;
-    if (!B->exec || B->captured != active) JB_TRY(batch_capture(B, active, eps, inner));
+    // the graph holds the fields' addresses and the sweep count: capture
+    // again when the active set, a field or inner changes
+    const bool same = B->exec && B->captured == active && B->captured_inner == inner &&
+                      std::equal(B->captured_eps.begin(), B->captured_eps.end(), eps);
+    if (!same) JB_TRY(batch_capture(B, active, eps, inner));
     if (step == 0) {
       // order the graph after the eager work on the caller's stream
       JB_CUDA(cudaEventRecord(B->events[B->nbranch + 1], st));

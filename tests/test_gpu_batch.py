@@ -81,3 +81,23 @@ def test_batch_reuses_graph_until_a_problem_leaves():
     assert batch.graph_launches <= 2
     with pytest.raises(ValueError):
         batch.run([np.eye(3)] * 2, tol=1e-6)
+
+
+@pytest.mark.gpu
+def test_batch_runs_again_on_new_fields():
+    """A second run with new strain fields (and another inner count) must not
+    reuse a graph captured for the first run's fields."""
+    probs = _problems(4, count=3)
+    ops_ = [_operators(p, "truncated") for p in probs]
+    batch = BatchedMixedScheme([(g, l, 3) for g, l in ops_], inner=10, branches=3)
+    first = batch.run([np.eye(3)] * 3, tol=1e-8, max_outer=500)
+    keep = [r.eps.clone() for r in first]
+    for r in first:
+        r.eps.fill_(float("nan"))
+    second = batch.run([np.eye(3)] * 3, tol=1e-8, max_outer=500)
+    for k, r in zip(keep, second):
+        assert torch.equal(k, r.eps)
+    third = batch.run([np.eye(3)] * 3, tol=1e-8, max_outer=500, inner=15)
+    for (g, l), r in zip(ops_, third):
+        one = MixedScheme(g, l, 3, inner=15).run(np.eye(3), tol=1e-8, max_outer=500)
+        assert torch.equal(one.eps, r.eps)
