@@ -127,6 +127,15 @@ int jb_green_apply(jb_green *green, const void *x, void *y, int64_t batch,
 int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
                            double nu, int variant, const double *x, double *y,
                            void *stream);
+/* Column-pass tile schedule of this operator (no reference counterpart; the
+ * reference plans with FFTW).  v[6] = {plain width, plain input tiles, plain
+ * compile-time tiles allowed, Green width, Green input tiles, Green
+ * compile-time tiles allowed}; widths in complex columns (the Green one a
+ * multiple of s), input tiles 2 or 3, 0 = built-in rule.  A width whose
+ * tiles do not fit the shared-memory budget is narrowed.  Set by the
+ * autotuner (janus_b200.autotune) from timed candidates. */
+int jb_green_set_tuning(jb_green *green, const int *v, int count);
+int jb_green_get_tuning(jb_green *green, int *v, int count);
 /* set_frequency + to_memoryview at index b (green.pyx:146-171, 312-342 and
  * the subclasses' c_set_frequency / c_to_memoryview): host, FP64, with the
  * reference's range checks (0 <= b_i < n_i). */

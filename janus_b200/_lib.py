@@ -49,6 +49,8 @@ _SIGS = {
     "jb_green_create": ([c_int, P_int64, c_double, c_double, c_double, c_int, c_int,
                          ctypes.POINTER(c_void_p)], c_int),
     "jb_green_destroy": ([c_void_p], c_int),
+    "jb_green_set_tuning": ([c_void_p, P_int, c_int], c_int),
+    "jb_green_get_tuning": ([c_void_p, P_int, c_int], c_int),
     "jb_green_apply": ([c_void_p, c_void_p, c_void_p, c_int64, c_void_p], c_int),
     "jb_green_matrix": ([c_void_p, P_int32, P_double], c_int),
     "jb_green_apply_by_freq": ([c_void_p, P_int32, P_double, P_double], c_int),

@@ -255,6 +255,7 @@ struct jb_green_s {
   DeviceBuf spec;
   DeviceBuf bidx;
   DeviceBuf mnbuf;        // per-coefficient M/N table, built on first use
+  jb::ColsTuning tune_plain, tune_green;  // column-pass schedules (autotuner)
   bool use_table = true;  // false: evaluate the operator on the fly
 };
 
@@ -373,19 +374,19 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
   rec->mark(st);
   if (dim == 3) {
     JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 0, L * n0, m * C, spec, spec, C,
-                                         dim, nullptr, n1, m, st),
+                                         dim, nullptr, n1, m, st, &g->tune_plain),
                          "cols_fwd_axis1"));
     rec->mark(st);
   }
   const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
   JB_TRY(green_prepare(g, st));
   JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
-                                       &g->gt, n1, m, st),
+                                       &g->gt, n1, m, st, &g->tune_green),
                        "cols_green_axis0"));
   rec->mark(st);
   if (dim == 3) {
     JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 1, L * n0, m * C, spec, spec, C,
-                                         dim, nullptr, n1, m, st),
+                                         dim, nullptr, n1, m, st, &g->tune_plain),
                          "cols_inv_axis1"));
     rec->mark(st);
   }
@@ -649,6 +650,35 @@ int jb_green_destroy(jb_green* G) {
   if (G->bidx.p) cudaFree(G->bidx.p);
   if (G->mnbuf.p) cudaFree(G->mnbuf.p);
   delete G;
+  return JB_OK;
+}
+
+int jb_green_set_tuning(jb_green* G, const int* v, int count) {
+  if (!G || !v) return fail(JB_EINVAL, "NULL argument");
+  if (count != 6) return fail(JB_EINVAL, "tuning takes 6 values");
+  const int C = G->dim == 2 ? 3 : 6;
+  if (v[0] < 0 || v[0] > 128 || v[3] < 0 || v[3] > 128 || (v[3] % C) != 0)
+    return fail(JB_EINVAL, "tile widths must be in [0, 128], the Green one a multiple of s");
+  for (int k : {v[1], v[4]})
+    if (k != 0 && k != 2 && k != 3) return fail(JB_EINVAL, "input tiles must be 0, 2 or 3");
+  G->tune_plain.w = v[0];
+  G->tune_plain.nbuf = v[1];
+  G->tune_plain.ct = v[2] != 0;
+  G->tune_green.w = v[3];
+  G->tune_green.nbuf = v[4];
+  G->tune_green.ct = v[5] != 0;
+  return JB_OK;
+}
+
+int jb_green_get_tuning(jb_green* G, int* v, int count) {
+  if (!G || !v) return fail(JB_EINVAL, "NULL argument");
+  if (count != 6) return fail(JB_EINVAL, "tuning takes 6 values");
+  v[0] = G->tune_plain.w;
+  v[1] = G->tune_plain.nbuf;
+  v[2] = G->tune_plain.ct;
+  v[3] = G->tune_green.w;
+  v[4] = G->tune_green.nbuf;
+  v[5] = G->tune_green.ct;
   return JB_OK;
 }
 

@@ -1163,15 +1163,12 @@ int persistent_grid(K kernel, int threads, size_t smem, int64_t tiles) {
 // tile width and shared memory of the tensor-TMA column kernel: two input
 // tiles and one compute partner of n x W complex, 128-byte aligned
 bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem, int* nbuf,
-                    bool stage_ax0 = true) {
+                    bool stage_ax0, const ColsTuning* tune) {
   const size_t cs = dtype == F64 ? 16 : 8;
-  // measured on B200 (128^3 x 6, FP64): W = 8 columns for plain passes,
-  // 12 (two 6-component coefficients) for the Green pass
+  // built-in rule, measured on B200 (128^3 x 6, FP64): W = 8 columns for
+  // plain passes, 12 (two 6-component coefficients) for the Green pass
   int w = unit == 1 ? 8 : unit * (12 / unit > 0 ? 12 / unit : 1);
-  if (const char* env = getenv("JB_COLS_W")) {
-    const int v = atoi(env);
-    if (v >= unit && v % unit == 0 && v <= 128) w = v;
-  }
+  if (tune && tune->w >= unit && tune->w % unit == 0 && tune->w <= 128) w = tune->w;
   if (w < unit) w = unit;
   for (;; w -= unit) {
     // + the axis-0 Green values (4 reals per row, unless tabulated) and alignment
@@ -1183,7 +1180,7 @@ bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem, int* nbuf,
     // on B200, 128^3 x 6: FP32 plain passes 8% faster with three; FP64
     // slower, the third tile costing a resident CTA)
     int nb = dtype == F32 ? 3 : 2;
-    if (const char* env = getenv("JB_COLS_NBUF")) nb = atoi(env) == 3 ? 3 : 2;
+    if (tune && (tune->nbuf == 2 || tune->nbuf == 3)) nb = tune->nbuf;
     if (bytes_for(nb) > kPipeBudget) nb = 2;
     const size_t bytes = bytes_for(nb);
     if (bytes <= kPipeBudget || w <= unit) {
@@ -1507,7 +1504,7 @@ cudaError_t cols_tma_launch(const CUtensorMap& tin, const CUtensorMap& tout,
 template <typename T>
 cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, const void* in,
                    void* out, int C, int dim, const GreenDeviceTables* gt, int64_t m_last,
-                   cudaStream_t st) {
+                   cudaStream_t st, const ColsTuning* tune) {
   ColsArgs<T> a{};
   int W;
   size_t smem;
@@ -1533,7 +1530,7 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     const size_t cs = sizeof(cx<T>);
     if (al16(in) && al16(out) && (inner * cs) % 16 == 0 &&
         cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &Wp, &sp, &nbuf,
-                       mode == 2 && a.mn == nullptr)) {
+                       mode == 2 && a.mn == nullptr, tune)) {
       int nbox = n <= 256 ? n : 256;  // rows per box: largest divisor of n up to 256
       while (n % nbox != 0) --nbox;
       CUtensorMap tin, tout;
@@ -1546,7 +1543,7 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
         const int thr = tile_threads(Wp);
         const int64_t tiles = (inner + Wp - 1) / Wp * outer;
         const bool ct_w = Wp == (mode == 2 ? 12 : 8) && (mode != 2 || C == 3 || C == 6);
-        if (ct_w && !getenv("JB_NO_CT")) {
+        if (ct_w && (!tune || tune->ct)) {
           if (n == 64) return cols_ct_dispatch<T, 64>(mode, dim, tin, tout, b, nbox, sp, tiles, st);
           if (n == 128)
             return cols_ct_dispatch<T, 128>(mode, dim, tin, tout, b, nbox, sp, tiles, st);
@@ -1596,10 +1593,11 @@ cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const v
 cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer, int64_t inner,
                         const void* in, void* out, int C, int dim,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
-                        cudaStream_t st) {
+                        cudaStream_t st, const ColsTuning* tune) {
   (void)n1;
-  return dtype == F64 ? cols_t<double>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st)
-                      : cols_t<float>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st);
+  return dtype == F64
+             ? cols_t<double>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st, tune)
+             : cols_t<float>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st, tune);
 }
 
 cudaError_t launch_local(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,

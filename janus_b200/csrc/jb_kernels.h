@@ -80,13 +80,23 @@ cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const v
 cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const void* in,
                             void* y, const RealGeom& g, double scale,
                             const UpdateDesc* upd, int* nblocks_out, cudaStream_t st);
+// tile schedule of a column pass (0 = the built-in rule): tile width in
+// complex columns (a multiple of the coefficient size for the Green pass),
+// rotating input tiles (2 or 3), and whether compile-time FFT tiles may be
+// used where they exist.  Chosen per operator by the autotuner.
+struct ColsTuning {
+  int w = 0;
+  int nbuf = 0;
+  int ct = 1;
+};
+
 // complex transform along a strided axis of [outer][n][inner] (complex units).
 // mode 0: forward, 1: inverse, 2: forward -> Green contraction -> inverse
 // (axis 0 only; dim/m_last/grid describe the spectrum for the contraction).
 cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer,
                         int64_t inner, const void* in, void* out, int C, int dim,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
-                        cudaStream_t st);
+                        cudaStream_t st, const ColsTuning* tune = nullptr);
 // M/N table of the Green operator on the half spectrum of an n0 x n1 (x n2)
 // grid: table[(f12 * n0 + b0) * NT + c], f12 = b1 * m + b2 (3D) or b1 (2D),
 // NT = 21 (3D) / 8 (2D).  `out` has n0 * n1 * m * NT (3D) reals of the dtype.
