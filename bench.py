@@ -266,6 +266,10 @@ def run_gpu(args, rank, world, dist):
     n = args.n
     phase, tens, green, E = build_problem(n, 2024 + rank, args.variant, dtype)
     loc = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dtype)
+    tuning = None
+    if not args.no_tune:
+        from janus_b200 import autotune
+        tuning = autotune.tune(green, loc, nload=6, use_cache=False)
     solver = BasicScheme(green, loc, nload=6)
     solver.set_load(E)
     eps = solver.new_field()
@@ -418,7 +422,7 @@ def run_gpu(args, rank, world, dist):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": nrec * len(passes),
             "passes_ms_per_step": {k: round(v / max(nrec, 1), 4) for k, v in passes.items()},
-            "clocks": clocks, "solve": solve,
+            "clocks": clocks, "solve": solve, "tuning": tuning,
         }
         print(json.dumps(line), flush=True)
 
@@ -555,6 +559,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the column-schedule autotuner (built-in rules)")
     ap.add_argument("--workload", default="spheres3d", choices=["spheres3d", "batch2d"],
                     help="spheres3d: the headline step; batch2d: batched 2D cells")
     ap.add_argument("--batch-count", type=int, default=64)
