@@ -50,6 +50,28 @@ def pass_bytes(s, p, m=1):
             "rows_c2r_update": 3 * s * p, "reduce_residual": 0}
 
 
+def reduce_max(x, dist, device="cuda"):
+    """Max of a per-rank float over all ranks (the job's time is its slowest
+    rank); identity without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_step, steps, ms):
+    """Units processed by all ranks per second: every rank runs its own
+    replica of the workload (weak scaling), timed as the slowest rank."""
+    return world * units_per_step * steps / (ms / 1e3)
+
+
+def replica_seed(rank):
+    """Seed of the microstructure rank `rank` solves (independent replicas)."""
+    return 2024 + rank
+
+
 def env_int(name, default):
     try:
         return int(os.environ.get(name, default))
@@ -264,7 +286,7 @@ def run_gpu(args, rank, world, dist):
     torch.cuda.set_device(local)
     dtype = torch.float64 if args.dtype == "f64" else torch.float32
     n = args.n
-    phase, tens, green, E = build_problem(n, 2024 + rank, args.variant, dtype)
+    phase, tens, green, E = build_problem(n, replica_seed(rank), args.variant, dtype)
     loc = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dtype)
     tuning = None
     if not args.no_tune:
@@ -300,12 +322,9 @@ def run_gpu(args, rank, world, dist):
     ms = start.elapsed_time(end)
     passes, nrec = solver.timing_end()
     clocks = sampler.stop()
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, dist)
     vox_step = 6 * n ** 3
-    value = world * vox_step * args.steps / (ms / 1e3)
+    value = whole_job_rate(world, vox_step, args.steps, ms)
 
     # roofline of the dominant pass (algorithmic bytes / its mean duration)
     p = 8 if dtype == torch.float64 else 4
@@ -351,11 +370,8 @@ def run_gpu(args, rank, world, dist):
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         e2e_ms = max(s0.elapsed_time(s1), wall * 1e3)
-        if dist is not None:
-            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        e2e = {"value": world * vox_step * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+        e2e_ms = reduce_max(e2e_ms, dist)
+        e2e = {"value": whole_job_rate(world, vox_step, args.steps, e2e_ms), "unit": UNIT,
                "h2d_bytes_per_step": int((phase.nbytes + E.nbytes) / args.steps),
                "d2h_bytes_per_step": int((out.numel() * out.element_size()) / args.steps
                                          + 6 * 8),
