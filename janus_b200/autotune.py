@@ -44,7 +44,8 @@ def candidates(dim, dtype):
     """(plain, green) candidate lists of (width, input tiles, compile-time)."""
     s = 3 if dim == 2 else 6
     plain = [(w, nb, 1) for w in (4, 8, 16) for nb in (2, 3)] + [(8, 2, 0), (8, 3, 0)]
-    green = [(w, nb, 1) for w in (s, 2 * s, 3 * s) for nb in (2, 3)] + [(2 * s, 2, 0)]
+    green = [(w, nb, 1) for w in (s, 2 * s, 3 * s) for nb in (2, 3)] + [(s, 2, 0),
+                                                                          (2 * s, 2, 0)]
     return (plain if dim == 3 else []), green
 
 

@@ -92,6 +92,14 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
+// threads of a tile kernel: those of its compile-time FFT tile, else kThreads
+template <int NCT, int WCT> constexpr int tile_max_threads() {
+  if constexpr (NCT > 0)
+    return ct_threads<NCT, WCT>();
+  else
+    return kThreads;
+}
+
 template <typename T> struct RowsArgs {
   const T* x;
   cx<T>* out;
@@ -192,7 +200,7 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* fail_flag) {
 //  4. split into the two half spectra, staged as [rr][k][c] and written out
 //     by one bulk copy.
 template <typename T, int CC, bool LOCAL, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
+__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>()) rows_r2c_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -349,13 +357,13 @@ __global__ void __launch_bounds__(kThreads) rows_r2c_kernel(RowsArgs<T> a) {
 enum { kEpiPlain = 0, kEpiUpdate = 1, kEpiResid = 2, kEpiRhs = 3 };
 
 template <typename T, int CC, int EPI, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(kThreads) rows_c2r_kernel(RowsArgs<T> a) {
+__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>()) rows_c2r_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   using OT = typename std::conditional<EPI == kEpiResid, float, T>::type;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int fail_flag;
-  __shared__ double red[kThreads / 32];
+  __shared__ double red[tile_max_threads<NCT, WCT>() / 32];
   constexpr int kC = CC;
   constexpr bool kSide = EPI != kEpiPlain;
   const int n = NCT > 0 ? NCT : a.plan.n;
@@ -687,15 +695,9 @@ template <typename P> __device__ __forceinline__ P* align128_ptr(void* p) {
 template <typename T, int MODE, int NCT> constexpr int cols_min_blocks() {
   return (MODE == 2 && NCT > 0) ? (sizeof(T) == 8 ? 2 : 4) : 1;
 }
-template <int NCT, int WCT> constexpr int cols_max_threads() {
-  if constexpr (NCT > 0)
-    return ct_threads<NCT, WCT>();
-  else
-    return kThreads;
-}
 
 template <typename T, int MODE, int DIM, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(cols_max_threads<NCT, WCT>(), cols_min_blocks<T, MODE, NCT>())
+__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<T, MODE, NCT>())
     cols_tma_kernel(const __grid_constant__ CUtensorMap tin,
                     const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
   using C = cx<T>;
@@ -1485,6 +1487,13 @@ cudaError_t cols_ct_dispatch(int mode, int dim, const CUtensorMap& tin, const CU
                              cudaStream_t st) {
   if (mode == 0) return cols_ct_launch<T, 0, 2, N, 8>(tin, tout, a, nbox, smem, tiles, st);
   if (mode == 1) return cols_ct_launch<T, 1, 2, N, 8>(tin, tout, a, nbox, smem, tiles, st);
+  if constexpr (N == 256) {
+    // six-column Green tiles: the width FP64 tiles of 256 rows fit
+    if (a.W == 6) {
+      if (dim == 2) return cols_ct_launch<T, 2, 2, N, 6>(tin, tout, a, nbox, smem, tiles, st);
+      return cols_ct_launch<T, 2, 3, N, 6>(tin, tout, a, nbox, smem, tiles, st);
+    }
+  }
   if (dim == 2) return cols_ct_launch<T, 2, 2, N, 12>(tin, tout, a, nbox, smem, tiles, st);
   return cols_ct_launch<T, 2, 3, N, 12>(tin, tout, a, nbox, smem, tiles, st);
 }
@@ -1542,7 +1551,8 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
         b.nbuf = nbuf;
         const int thr = tile_threads(Wp);
         const int64_t tiles = (inner + Wp - 1) / Wp * outer;
-        const bool ct_w = Wp == (mode == 2 ? 12 : 8) && (mode != 2 || C == 3 || C == 6);
+        const bool ct_w = (mode == 2 ? (Wp == 12 || (Wp == 6 && n == 256)) : Wp == 8) &&
+                          (mode != 2 || C == 3 || C == 6);
         if (ct_w && (!tune || tune->ct)) {
           if (n == 64) return cols_ct_dispatch<T, 64>(mode, dim, tin, tout, b, nbox, sp, tiles, st);
           if (n == 128)

@@ -14,17 +14,21 @@ from oracle import janus_oracle as O
 def _green(dim, n, variant, dtype):
     mat = material.create(0.75, 0.3, dim)
     f = filtered if variant == "filtered" else truncated
-    return f(mat.green_operator(), (n,) * dim, 1.0, dtype=dtype)
+    shape = (n,) * dim if np.isscalar(n) else tuple(n)
+    return f(mat.green_operator(), shape, 1.0, dtype=dtype)
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("dim,n,dtype", [(3, 32, torch.float64), (3, 64, torch.float32),
-                                         (2, 64, torch.float64), (2, 96, torch.float32)])
+                                         (2, 64, torch.float64), (2, 96, torch.float32),
+                                         (2, 256, torch.float64),
+                                         (3, (256, 16, 16), torch.float64),
+                                         (3, (256, 16, 16), torch.float32)])
 def test_every_candidate_computes_the_same_operator(dim, n, dtype):
     g = _green(dim, n, "filtered", dtype)
     s = g.ishape[-1]
     rng = np.random.default_rng(0)
-    x = torch.from_numpy(rng.standard_normal((n,) * dim + (s,))).to("cuda", dtype)
+    x = torch.from_numpy(rng.standard_normal(tuple(g.ishape))).to("cuda", dtype)
     ref = g.apply(x).double().cpu().numpy()
     exact = O.green_apply(x.double().cpu().numpy(), 0.75, 0.3, 1.0, "filtered")
     tol = 1e-12 if dtype == torch.float64 else 2e-5
