@@ -100,6 +100,16 @@ template <int NCT, int WCT> constexpr int tile_max_threads() {
     return kThreads;
 }
 
+// resident CTAs per SM asked of the register allocator for the row kernels'
+// compile-time tiles of up to 192 threads (FP64: 4, at most 80 registers;
+// FP32: 6), so that registers never bound their occupancy below shared memory
+template <typename T, int NCT, int WCT> constexpr int rows_min_blocks() {
+  if constexpr (NCT > 0) {
+    if (ct_threads<NCT, WCT>() <= 192) return sizeof(T) == 8 ? 4 : 6;
+  }
+  return 1;
+}
+
 template <typename T> struct RowsArgs {
   const T* x;
   cx<T>* out;
@@ -200,7 +210,8 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* fail_flag) {
 //  4. split into the two half spectra, staged as [rr][k][c] and written out
 //     by one bulk copy.
 template <typename T, int CC, bool LOCAL, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>()) rows_r2c_kernel(RowsArgs<T> a) {
+__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<T, NCT, WCT>())
+    rows_r2c_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -357,7 +368,8 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>()) rows_r2c_kernel(
 enum { kEpiPlain = 0, kEpiUpdate = 1, kEpiResid = 2, kEpiRhs = 3 };
 
 template <typename T, int CC, int EPI, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>()) rows_c2r_kernel(RowsArgs<T> a) {
+__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<T, NCT, WCT>())
+    rows_c2r_kernel(RowsArgs<T> a) {
   using C = cx<T>;
   using OT = typename std::conditional<EPI == kEpiResid, float, T>::type;
   extern __shared__ __align__(128) unsigned char smem[];
