@@ -64,6 +64,7 @@ _SIGS = {
                                c_int, c_void_p], c_int),
     "jb_local_gradient": ([c_int, c_int, c_int64, c_int, c_void_p, c_void_p, c_double,
                            c_void_p, c_void_p], c_int),
+    "jb_mixed_set_method": ([c_void_p, c_int], c_int),
     "jb_batch_create": ([c_int, ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)],
                         c_int),
     "jb_batch_destroy": ([c_void_p], c_int),

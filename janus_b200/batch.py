@@ -27,10 +27,11 @@ class BatchedMixedScheme:
     """problems: sequence of (green_op, local_op, nload) triples (FP64
     operators of janus_b200.green / operators, any grid size each)."""
 
-    def __init__(self, problems, inner=20, branches=8):
+    def __init__(self, problems, inner=20, branches=8, method="basic"):
         if not problems:
             raise ValueError("a batch needs at least one problem")
-        self.schemes = [MixedScheme(g, l, nload, inner) for g, l, nload in problems]
+        self.schemes = [MixedScheme(g, l, nload, inner, method=method)
+                        for g, l, nload in problems]
         self.inner = int(inner)
         handles = (ctypes.c_void_p * len(self.schemes))(
             *[s._handle.value for s in self.schemes])

@@ -390,8 +390,18 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
                          "cols_inv_axis1"));
     rec->mark(st);
   }
-  JB_TRY(launch_status(jb::launch_rows_c2r(g->dtype, last, C, (int)L, spec, y, geom,
-                                           1.0 / (double)N, upd, nb_rows, st),
+  // mode 4 (x + Gamma0[..]): the right-hand-side epilogue rhs - scale*y with
+  // a negative scale
+  double scale = 1.0 / (double)N;
+  jb::UpdateDesc add;
+  if (upd && upd->mode == 4) {
+    add = *upd;
+    add.mode = 3;
+    upd = &add;
+    scale = -scale;
+  }
+  JB_TRY(launch_status(jb::launch_rows_c2r(g->dtype, last, C, (int)L, spec, y, geom, scale, upd,
+                                           nb_rows, st),
                        "rows_c2r"));
   rec->mark(st);
   return JB_OK;
@@ -1231,7 +1241,9 @@ struct jb_mixed_s {
   jb_green* g32 = nullptr;
   jb_local* l32 = nullptr;
   int L = 1;
+  int method = JB_INNER_BASIC;
   DeviceBuf spec, partials, E, res, normd, r32, d32, mean;
+  DeviceBuf kr_rh, kr_p, kr_v, kr_s, kr_t, kr_r, kr_part, kr_state;  // BiCGSTAB
   std::vector<double> norm;
 };
 
@@ -1278,10 +1290,19 @@ extern "C" int jb_mixed_create(jb_green* g64, jb_local* l64, jb_green* g32, jb_l
   return JB_OK;
 }
 
+extern "C" int jb_mixed_set_method(jb_mixed* M, int method) {
+  if (!M) return fail(JB_EINVAL, "NULL argument");
+  if (method != JB_INNER_BASIC && method != JB_INNER_BICGSTAB)
+    return fail(JB_EINVAL, "method must be JB_INNER_BASIC or JB_INNER_BICGSTAB");
+  M->method = method;
+  return JB_OK;
+}
+
 extern "C" int jb_mixed_destroy(jb_mixed* M) {
   if (!M) return JB_OK;
   for (DeviceBuf* b : {&M->spec, &M->partials, &M->E, &M->res, &M->normd, &M->r32, &M->d32,
-                       &M->mean})
+                       &M->mean, &M->kr_rh, &M->kr_p, &M->kr_v, &M->kr_s, &M->kr_t, &M->kr_r,
+                       &M->kr_part, &M->kr_state})
     if (b->p) cudaFree(b->p);
   delete M;
   return JB_OK;
@@ -1352,6 +1373,75 @@ int mixed_correct(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
                        "axpy");
 }
 
+// correction by `inner` BiCGSTAB iterations on A d = r (FP32, A d = d +
+// Gamma0[(C - C0):d], from d = 0), eps += d
+// the BiCGSTAB work fields and scalars (allocated on first use, before any
+// graph capture)
+int mixed_krylov_buffers(jb_mixed* M) {
+  const int C = M->g64->dim == 2 ? 3 : 6;
+  const int L = M->L;
+  const int64_t nel = M->l64->nvox * C;
+  const size_t fb = sizeof(float) * (size_t)L * nel;
+  for (DeviceBuf* b : {&M->kr_rh, &M->kr_p, &M->kr_v, &M->kr_s, &M->kr_t, &M->kr_r})
+    JB_TRY(ensure_buf(*b, fb));
+  JB_TRY(ensure_buf(M->kr_part, sizeof(double) * 2 * L * jb::krylov_blocks(nel, L)));
+  return ensure_buf(M->kr_state, sizeof(jb::KrylovState) * L);
+}
+
+int mixed_correct_bicgstab(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
+  const int C = M->g64->dim == 2 ? 3 : 6;
+  const int L = M->L;
+  const int64_t nel = M->l64->nvox * C;
+  const size_t fb = sizeof(float) * (size_t)L * nel;
+  JB_TRY(mixed_krylov_buffers(M));
+  jb::LocalDesc loc32 = local_desc(M->l32);
+  float* x = static_cast<float*>(M->d32.p);
+  float* b = static_cast<float*>(M->r32.p);
+  float *rh = static_cast<float*>(M->kr_rh.p), *p = static_cast<float*>(M->kr_p.p),
+        *v = static_cast<float*>(M->kr_v.p), *s = static_cast<float*>(M->kr_s.p),
+        *t = static_cast<float*>(M->kr_t.p), *r = static_cast<float*>(M->kr_r.p);
+  double* part = static_cast<double*>(M->kr_part.p);
+  auto* ks = static_cast<jb::KrylovState*>(M->kr_state.p);
+  JB_CUDA(cudaMemsetAsync(x, 0, fb, st));
+  JB_CUDA(cudaMemsetAsync(p, 0, fb, st));
+  JB_CUDA(cudaMemsetAsync(v, 0, fb, st));
+  JB_CUDA(cudaMemcpyAsync(r, b, fb, cudaMemcpyDeviceToDevice, st));
+  JB_CUDA(cudaMemcpyAsync(rh, b, fb, cudaMemcpyDeviceToDevice, st));
+  JB_TRY(launch_status(jb::launch_krylov_dot(F32, nel, L, rh, r, nullptr, nullptr, part, st),
+                       "krylov_dot"));
+  JB_TRY(launch_status(jb::launch_krylov_scalars(0, nel, L, part, ks, st), "krylov_scalars"));
+  auto apply = [&](const float* in, float* out) {
+    jb::UpdateDesc u;
+    u.mode = 4;  // out = in + Gamma0[(C - C0):in]
+    u.eps = out;
+    u.rhs = in;
+    return green_passes(M->g32, in, out, L, M->spec.p, &loc32, &u, nullptr, st);
+  };
+  for (int it = 0; it < inner; ++it) {
+    JB_TRY(launch_status(
+        jb::launch_krylov_update(F32, 0, nel, L, p, nullptr, nullptr, v, r, nullptr, ks, nullptr,
+                                 st),
+        "krylov_p"));
+    JB_TRY(apply(p, v));
+    JB_TRY(launch_status(jb::launch_krylov_dot(F32, nel, L, rh, v, nullptr, nullptr, part, st),
+                         "krylov_dot"));
+    JB_TRY(launch_status(jb::launch_krylov_scalars(1, nel, L, part, ks, st), "krylov_scalars"));
+    JB_TRY(launch_status(
+        jb::launch_krylov_update(F32, 1, nel, L, s, nullptr, nullptr, v, r, nullptr, ks, nullptr,
+                                 st),
+        "krylov_s"));
+    JB_TRY(apply(s, t));
+    JB_TRY(launch_status(jb::launch_krylov_dot(F32, nel, L, t, s, t, t, part, st), "krylov_dot"));
+    JB_TRY(launch_status(jb::launch_krylov_scalars(2, nel, L, part, ks, st), "krylov_scalars"));
+    JB_TRY(launch_status(
+        jb::launch_krylov_update(F32, 2, nel, L, x, p, s, t, r, rh, ks, part, st), "krylov_xr"));
+    JB_TRY(launch_status(jb::launch_krylov_scalars(3, nel, L, part, ks, st), "krylov_scalars"));
+  }
+  return launch_status(jb::launch_axpy_f32_to_f64((int64_t)L * nel, x, static_cast<double*>(eps),
+                                                  st),
+                       "axpy");
+}
+
 // mean of (C - C0):eps per load case and component into host mean_tau
 int mixed_mean(jb_mixed* M, const void* eps, double* mean_tau, cudaStream_t st) {
   const int C = M->g64->dim == 2 ? 3 : 6;
@@ -1395,8 +1485,13 @@ extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, i
       ++outer;
       break;
     }
-    JB_TRY(mixed_correct(M, eps, inner, st));
-    fp32 += inner - 1;
+    if (M->method == JB_INNER_BICGSTAB) {
+      JB_TRY(mixed_correct_bicgstab(M, eps, inner, st));
+      fp32 += 2 * inner;
+    } else {
+      JB_TRY(mixed_correct(M, eps, inner, st));
+      fp32 += inner - 1;
+    }
   }
   if (outer_out) *outer_out = outer;
   if (fp32_iters_out) *fp32_iters_out = fp32;
@@ -1499,7 +1594,9 @@ int batch_capture(jb_batch* B, const std::vector<char>& active, void* const* eps
   for (size_t i = 0; i < B->prob.size() && r == JB_OK && e == cudaSuccess; ++i) {
     if (!active[i]) continue;
     cudaStream_t st = B->streams[B->branch[i] + 1];
-    r = mixed_correct(B->prob[i], eps[i], inner, st);
+    r = B->prob[i]->method == JB_INNER_BICGSTAB
+            ? mixed_correct_bicgstab(B->prob[i], eps[i], inner, st)
+            : mixed_correct(B->prob[i], eps[i], inner, st);
     if (r == JB_OK) r = mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st);
   }
   for (int k = 0; k < B->nbranch && e == cudaSuccess; ++k) {
@@ -1559,6 +1656,7 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
   }
   for (size_t i = 0; i < P; ++i) {
     JB_TRY(green_prepare(B->prob[i]->g32, st));  // nothing lazily built inside a capture
+    if (B->prob[i]->method == JB_INNER_BICGSTAB) JB_TRY(mixed_krylov_buffers(B->prob[i]));
     JB_TRY(mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st));
   }
   std::vector<double> rh(B->nres);
@@ -1612,7 +1710,9 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
     jb_mixed* M = B->prob[i];
     const int C = M->g64->dim == 2 ? 3 : 6;
     if (outer_out) outer_out[i] = outer[i];
-    if (fp32_iters_out) fp32_iters_out[i] = (outer[i] - 1) * (inner - 1);
+    if (fp32_iters_out)
+      fp32_iters_out[i] =
+          (outer[i] - 1) * (M->method == JB_INNER_BICGSTAB ? 2 * inner : inner - 1);
     if (mean_tau) JB_TRY(mixed_mean(M, eps[i], mean_tau + eoff, st));
     eoff += (size_t)M->L * C;
   }

@@ -62,6 +62,26 @@ struct UpdateDesc {
   float* rout = nullptr;        // mode 2
 };
 
+// BiCGSTAB scalars of one load case (device); active: 1 iterating, 2 last
+// update pending, 0 frozen (converged or broken down)
+struct KrylovState {
+  double rho, alpha, omega, rho1;
+  int active;
+};
+// blocks per load case of the Krylov vector kernels (partials per dot)
+int krylov_blocks(int64_t nel, int L);
+// partials[(l*2+q)*nb+b]: q 0 = a.b, q 1 = c.d (c may be NULL), per load case
+cudaError_t launch_krylov_dot(int dtype, int64_t nel, int L, const void* a, const void* b,
+                              const void* c, const void* d, double* partials, cudaStream_t st);
+// stage 0: init + rho1, 1: alpha, 2: omega, 3: rho1 after the x/r update
+cudaError_t launch_krylov_scalars(int stage, int64_t nel, int L, const double* partials,
+                                  KrylovState* state, cudaStream_t st);
+// which 0: x(=p) = r + beta (x - omega t(=v)); 1: x(=s) = r - alpha t(=v);
+// 2: x += alpha p + omega s, r = s - omega t, partials of rh.r
+cudaError_t launch_krylov_update(int dtype, int which, int64_t nel, int L, void* x, const void* p,
+                                 const void* s, const void* t, void* r, const void* rh,
+                                 const KrylovState* state, double* partials, cudaStream_t st);
+
 // y[i] += (double) d[i] over n elements (FP64 field, FP32 correction)
 cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStream_t st);
 // y[i] = (float) x[i]

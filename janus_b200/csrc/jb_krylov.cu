@@ -1,0 +1,234 @@
+// Vector kernels of the BiCGSTAB inner solver of the mixed-precision scheme:
+// batched over load cases (fields [L][nel] back to back, one set of scalars
+// per load case, all scalars kept on the device so that an iteration needs no
+// host round trip).  Dot products accumulate in FP64 with per-block partial
+// sums reduced in a fixed order (deterministic).
+//
+// BiCGSTAB (van der Vorst 1992), per load case, for A x = b from x = 0:
+//   r = b, rh = b, rho = alpha = omega = 1, rho1 = rh.r, v = p = 0
+//   repeat: beta = (rho1/rho)(alpha/omega); p = r + beta (p - omega v)
+//           v = A p; alpha = rho1/(rh.v); rho = rho1; s = r - alpha v
+//           t = A s; omega = (t.s)/(t.t); x += alpha p + omega s
+//           r = s - omega t; rho1 = rh.r
+// A load case whose denominators vanish or stop being finite (breakdown or
+// exact convergence) is frozen: its x and r are left as they are.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "jb_kernels.h"
+
+namespace jb {
+namespace {
+
+constexpr int kKrThreads = 256;
+
+__device__ __forceinline__ double kr_block_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+  return s;
+}
+
+__device__ __forceinline__ bool kr_finite(double v) { return isfinite(v); }
+
+// partials[(l * 2 + q) * nb + b] of a.b (q = 0) and c.d (q = 1, if c)
+template <typename T>
+__global__ void __launch_bounds__(kKrThreads)
+    kr_dot_kernel(int64_t nel, const T* __restrict__ a, const T* __restrict__ b,
+                  const T* __restrict__ c, const T* __restrict__ d, double* partials) {
+  __shared__ double red[kKrThreads / 32];
+  const int l = blockIdx.y, nb = gridDim.x;
+  const int64_t off = (int64_t)l * nel;
+  double s0 = 0.0, s1 = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
+       i += (int64_t)nb * blockDim.x) {
+    s0 += (double)a[off + i] * (double)b[off + i];
+    if (c) s1 += (double)c[off + i] * (double)d[off + i];
+  }
+  s0 = kr_block_sum(s0, red);
+  if (threadIdx.x == 0) partials[((int64_t)l * 2) * nb + blockIdx.x] = s0;
+  if (c) {
+    s1 = kr_block_sum(s1, red);
+    if (threadIdx.x == 0) partials[((int64_t)l * 2 + 1) * nb + blockIdx.x] = s1;
+  }
+}
+
+// sum of the nb partials of dot q of load case blockIdx.x (fixed order)
+__device__ double kr_reduce(const double* partials, int nb, int q, double* red) {
+  const int l = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partials[((int64_t)l * 2 + q) * nb + b];
+  return kr_block_sum(s, red);
+}
+
+// stage 0: rho1 = rh.r after init; 1: alpha; 2: omega; 3: rho1 after x/r
+__global__ void __launch_bounds__(kKrThreads)
+    kr_scalar_kernel(int stage, const double* partials, int nb, KrylovState* st) {
+  __shared__ double red[kKrThreads / 32];
+  KrylovState& k = st[blockIdx.x];
+  const double s0 = kr_reduce(partials, nb, 0, red);
+  const double s1 = stage == 2 ? kr_reduce(partials, nb, 1, red) : 0.0;
+  if (threadIdx.x != 0) return;
+  if (stage == 0) {
+    k.rho = k.alpha = k.omega = 1.0;
+    k.rho1 = s0;
+    k.active = (s0 != 0.0 && kr_finite(s0)) ? 1 : 0;
+  } else if (stage == 1) {
+    if (k.active && s0 != 0.0 && kr_finite(k.rho1 / s0)) {
+      k.alpha = k.rho1 / s0;
+      k.rho = k.rho1;
+    } else {
+      k.active = 0;
+    }
+  } else if (stage == 2) {
+    // s1 = t.t, s0 = t.s
+    if (k.active) {
+      if (s1 != 0.0 && kr_finite(s0 / s1)) {
+        k.omega = s0 / s1;
+      } else {
+        k.omega = 0.0;  // t = 0: s solves it; finish with x += alpha p, r = s
+        k.active = 2;   // last update, then frozen
+      }
+    }
+  } else {
+    if (k.active == 2 || k.omega == 0.0 || s0 == 0.0 || !kr_finite(s0)) {
+      k.active = 0;
+    } else if (k.active) {
+      k.rho1 = s0;
+    }
+  }
+}
+
+// p = r + beta (p - omega v)
+template <typename T>
+__global__ void kr_update_p_kernel(int64_t nel, const T* __restrict__ r, const T* __restrict__ v,
+                                   T* __restrict__ p, const KrylovState* st) {
+  const int l = blockIdx.y;
+  const KrylovState k = st[l];
+  if (k.active != 1) return;
+  const double beta = (k.rho1 / k.rho) * (k.alpha / k.omega);
+  const T b = (T)beta, om = (T)k.omega;
+  const int64_t off = (int64_t)l * nel;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[off + i] = r[off + i] + b * (p[off + i] - om * v[off + i]);
+}
+
+// s = r - alpha v
+template <typename T>
+__global__ void kr_update_s_kernel(int64_t nel, const T* __restrict__ r, const T* __restrict__ v,
+                                   T* __restrict__ s, const KrylovState* st) {
+  const int l = blockIdx.y;
+  const KrylovState k = st[l];
+  if (k.active != 1) return;
+  const T a = (T)k.alpha;
+  const int64_t off = (int64_t)l * nel;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s[off + i] = r[off + i] - a * v[off + i];
+}
+
+// x += alpha p + omega s; r = s - omega t; partials of rh.r
+template <typename T>
+__global__ void __launch_bounds__(kKrThreads)
+    kr_update_xr_kernel(int64_t nel, T* __restrict__ x, const T* __restrict__ p,
+                        const T* __restrict__ s, const T* __restrict__ t, T* __restrict__ r,
+                        const T* __restrict__ rh, const KrylovState* st, double* partials) {
+  __shared__ double red[kKrThreads / 32];
+  const int l = blockIdx.y, nb = gridDim.x;
+  const KrylovState k = st[l];
+  const int64_t off = (int64_t)l * nel;
+  double acc = 0.0;
+  if (k.active != 0) {
+    const T a = (T)k.alpha, om = (T)k.omega;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
+         i += (int64_t)nb * blockDim.x) {
+      x[off + i] += a * p[off + i] + om * s[off + i];
+      const T rn = s[off + i] - om * t[off + i];
+      r[off + i] = rn;
+      acc += (double)rh[off + i] * (double)rn;
+    }
+  }
+  acc = kr_block_sum(acc, red);
+  if (threadIdx.x == 0) partials[((int64_t)l * 2) * nb + blockIdx.x] = acc;
+}
+
+int kr_blocks(int64_t nel, int L) {
+  int64_t b = (nel + kKrThreads * 4 - 1) / (kKrThreads * 4);
+  const int64_t cap = (148 * 8 + L - 1) / L;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+int krylov_blocks(int64_t nel, int L) { return kr_blocks(nel, L); }
+
+cudaError_t launch_krylov_dot(int dtype, int64_t nel, int L, const void* a, const void* b,
+                              const void* c, const void* d, double* partials, cudaStream_t st) {
+  const dim3 grid((unsigned)kr_blocks(nel, L), (unsigned)L);
+  if (dtype == F64)
+    kr_dot_kernel<double><<<grid, kKrThreads, 0, st>>>(
+        nel, static_cast<const double*>(a), static_cast<const double*>(b),
+        static_cast<const double*>(c), static_cast<const double*>(d), partials);
+  else
+    kr_dot_kernel<float><<<grid, kKrThreads, 0, st>>>(
+        nel, static_cast<const float*>(a), static_cast<const float*>(b),
+        static_cast<const float*>(c), static_cast<const float*>(d), partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_krylov_scalars(int stage, int64_t nel, int L, const double* partials,
+                                  KrylovState* state, cudaStream_t st) {
+  kr_scalar_kernel<<<L, kKrThreads, 0, st>>>(stage, partials, kr_blocks(nel, L), state);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_krylov_update(int dtype, int which, int64_t nel, int L, void* x, const void* p,
+                                 const void* s, const void* t, void* r, const void* rh,
+                                 const KrylovState* state, double* partials, cudaStream_t st) {
+  const dim3 grid((unsigned)kr_blocks(nel, L), (unsigned)L);
+  if (dtype == F64) {
+    using T = double;
+    if (which == 0)
+      kr_update_p_kernel<T><<<grid, kKrThreads, 0, st>>>(nel, static_cast<const T*>(r),
+                                                         static_cast<const T*>(t),
+                                                         static_cast<T*>(x), state);
+    else if (which == 1)
+      kr_update_s_kernel<T><<<grid, kKrThreads, 0, st>>>(nel, static_cast<const T*>(r),
+                                                         static_cast<const T*>(t),
+                                                         static_cast<T*>(x), state);
+    else
+      kr_update_xr_kernel<T><<<grid, kKrThreads, 0, st>>>(
+          nel, static_cast<T*>(x), static_cast<const T*>(p), static_cast<const T*>(s),
+          static_cast<const T*>(t), static_cast<T*>(r), static_cast<const T*>(rh), state,
+          partials);
+  } else {
+    using T = float;
+    if (which == 0)
+      kr_update_p_kernel<T><<<grid, kKrThreads, 0, st>>>(nel, static_cast<const T*>(r),
+                                                         static_cast<const T*>(t),
+                                                         static_cast<T*>(x), state);
+    else if (which == 1)
+      kr_update_s_kernel<T><<<grid, kKrThreads, 0, st>>>(nel, static_cast<const T*>(r),
+                                                         static_cast<const T*>(t),
+                                                         static_cast<T*>(x), state);
+    else
+      kr_update_xr_kernel<T><<<grid, kKrThreads, 0, st>>>(
+          nel, static_cast<T*>(x), static_cast<const T*>(p), static_cast<const T*>(s),
+          static_cast<const T*>(t), static_cast<T*>(r), static_cast<const T*>(rh), state,
+          partials);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace jb

@@ -169,12 +169,18 @@ class MixedScheme:
 
     Every outer step evaluates the FP64 residual r = E - eps - Gamma0[(C -
     C0):eps] (whose normalised norm is the stopping test, as for
-    BasicScheme), runs ``inner - 1`` FP32 iterations d <- r - Gamma0[(C -
-    C0):d] from d = r, and adds d to the FP64 strain field.  The FP32
-    operators are built from the given FP64 ones (same material, grid,
-    discretisation and phase map)."""
+    BasicScheme), solves the correction equation d + Gamma0[(C - C0):d] = r
+    approximately in FP32 and adds d to the FP64 strain field.  The inner
+    solver is ``method="basic"`` (``inner - 1`` basic iterations from d = r)
+    or ``method="bicgstab"`` (``inner`` BiCGSTAB iterations from d = 0, the
+    Krylov route of the reference's examples/square_inclusion_scipy.py,
+    which hands the same operator to scipy's gmres).  The FP32 operators are
+    built from the given FP64 ones (same material, grid, discretisation and
+    phase map)."""
 
-    def __init__(self, green_op, local_op, nload=1, inner=20):
+    METHODS = {"basic": 0, "bicgstab": 1}
+
+    def __init__(self, green_op, local_op, nload=1, inner=20, method="basic"):
         if isinstance(local_op, _BlockDiagonalOperator):
             local = local_op.local
         else:
@@ -191,10 +197,14 @@ class MixedScheme:
                                       dtype=torch.float32)
         self.local32 = LocalPhaseOperator(local.dim, local.shape, local.phase, local.sph,
                                           local.dev, dtype=torch.float32)
+        if method not in self.METHODS:
+            raise ValueError("method must be 'basic' or 'bicgstab'")
+        self.method = method
         self._handle = ctypes.c_void_p()
         _lib.check(_lib.lib().jb_mixed_create(green_op.handle, local.handle, self.green32.handle,
                                               self.local32.handle, self.nload,
                                               ctypes.byref(self._handle)))
+        _lib.check(_lib.lib().jb_mixed_set_method(self._handle, self.METHODS[method]))
 
     def __del__(self):
         h = getattr(self, "_handle", None)

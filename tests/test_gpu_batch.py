@@ -101,3 +101,19 @@ def test_batch_runs_again_on_new_fields():
     for (g, l), r in zip(ops_, third):
         one = MixedScheme(g, l, 3, inner=15).run(np.eye(3), tol=1e-8, max_outer=500)
         assert torch.equal(one.eps, r.eps)
+
+
+@pytest.mark.gpu
+def test_batch_bicgstab_matches_one_by_one():
+    probs = _problems(5, count=4)
+    ops_ = [_operators(p, "filtered") for p in probs]
+    batch = BatchedMixedScheme([(g, l, 3) for g, l in ops_], inner=15, branches=2,
+                               method="bicgstab")
+    res = batch.run([np.eye(3)] * 4, tol=1e-9, max_outer=200)
+    for (g, l), r in zip(ops_, res):
+        one = MixedScheme(g, l, 3, inner=15, method="bicgstab").run(np.eye(3), tol=1e-9,
+                                                                    max_outer=200)
+        assert r.outer_iterations == one.outer_iterations
+        assert r.fp32_iterations == one.fp32_iterations
+        assert torch.equal(r.eps, one.eps)
+        assert r.residuals[-1].max() <= 1e-9

@@ -75,3 +75,60 @@ def test_mixed_rejects_fp32_operators():
                       dtype="float32")
     with pytest.raises(ValueError):
         MixedScheme(green, loc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["truncated", "filtered"])
+def test_mixed_bicgstab_matches_fp64_3d(variant):
+    """Krylov inner solver (BiCGSTAB on the basic scheme's own operator, as
+    the reference's examples/square_inclusion_scipy.py uses gmres): same FP64
+    residual and stopping test, same effective stiffness, far fewer
+    operator applications."""
+    phase, _ = micro.random_spheres(32, radius=4, volume_fraction=0.3, seed=3)
+    mats = [(1.0, 0.3), (100.0, 0.2)]
+    g0, nu0 = 50.5, 0.3
+    loc, green, pars = _problem(phase, mats, g0, nu0, variant)
+    E = np.eye(6)
+    tol = 1e-10
+    ref = BasicScheme(green, loc, nload=6).run(E, 5000, tol=tol)
+    kr = MixedScheme(green, loc, nload=6, inner=25, method="bicgstab").run(E, tol=tol,
+                                                                          max_outer=100)
+    assert kr.residuals[-1].max() <= tol
+    assert np.isfinite(kr.eps.cpu().numpy()).all()
+    mat0 = material.create(g0, nu0, 3)
+    c_ref = ref.mean_stress(mat0, E)
+    c_kr = kr.mean_stress(mat0, E)
+    assert np.abs(c_kr - c_ref).max() <= 1e-7 * np.abs(c_ref).max()
+    err = (ref.eps - kr.eps).abs().max().item() / ref.eps.abs().max().item()
+    assert err <= 1e-8
+    # fp32_iterations counts applications of the operator
+    assert kr.fp32_iterations < 0.5 * ref.iterations
+
+
+@pytest.mark.gpu
+def test_mixed_bicgstab_high_contrast_2d():
+    phase = micro.square_inclusion(128, side=64)
+    loc, green, pars = _problem(phase, [(1.0, 0.3), (1000.0, 0.3)], 500.5, 0.3, "truncated")
+    E = np.eye(3)
+    ref = BasicScheme(green, loc, nload=3).run(E, 50000, tol=1e-9)
+    kr = MixedScheme(green, loc, nload=3, inner=25, method="bicgstab").run(
+        E, tol=1e-9, max_outer=200)
+    mat0 = material.create(500.5, 0.3, 2)
+    c_ref = ref.mean_stress(mat0, E)
+    c_kr = kr.mean_stress(mat0, E)
+    assert kr.residuals[-1].max() <= 1e-9
+    assert np.abs(c_kr - c_ref).max() <= 1e-7 * np.abs(c_ref).max()
+    assert kr.fp32_iterations < 0.2 * ref.iterations
+
+
+@pytest.mark.gpu
+def test_mixed_bicgstab_homogeneous_cell_stays_finite():
+    """dC constant: the LS solution is E itself, the first residual is zero
+    and no Krylov scalar may turn into NaN."""
+    phase = np.zeros((32, 32), dtype=np.uint8)
+    loc, green, pars = _problem(phase, [(3.0, 0.3)], 5.5, 0.3, "filtered")
+    E = np.eye(3)
+    r = MixedScheme(green, loc, nload=3, inner=10, method="bicgstab").run(E, tol=1e-12,
+                                                                        max_outer=5)
+    assert np.isfinite(r.eps.cpu().numpy()).all()
+    assert np.abs(r.eps.cpu().numpy() - E.reshape(3, 1, 1, 3)).max() <= 1e-12
