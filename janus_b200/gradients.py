@@ -61,8 +61,10 @@ class StiffnessFieldProblem:
 
     mu0, nu0: reference medium (default: mid-range of the field, nu).
     variant: "truncated" or "filtered" Green operator; h: voxel size.
-    mixed: FP32 bulk iterations with FP64 defect correction every
-    ``inner`` iterations (else plain FP64); tol: relative residual.
+    mixed: FP32 bulk iterations with FP64 defect correction (else plain
+    FP64), the correction solved by ``inner_method`` ("bicgstab": ``inner``
+    BiCGSTAB iterations; "basic": ``inner - 1`` basic iterations); tol:
+    relative residual of the basic scheme (both paths stop on it).
     """
     nu: float = 0.3
     avg_eps: Optional[np.ndarray] = None
@@ -73,7 +75,8 @@ class StiffnessFieldProblem:
     tol: float = 1e-8
     max_iter: int = 20000
     mixed: bool = True
-    inner: int = 20
+    inner: int = 25
+    inner_method: str = "bicgstab"
     keep_strain: bool = True
     stats: list = field(default_factory=list)   # per solve: (kind, iterations, residual)
 
@@ -114,7 +117,8 @@ class _Cell:
         """Strain fields (nload, *grid, s) for the rows of E (FP64)."""
         prob = self.prob
         if prob.mixed:
-            res = MixedScheme(self.green, self.local, E.shape[0], prob.inner).run(
+            res = MixedScheme(self.green, self.local, E.shape[0], prob.inner,
+                              method=prob.inner_method).run(
                 E, tol=prob.tol, max_outer=max(1, prob.max_iter // max(prob.inner, 1)))
             its = res.fp32_iterations + res.outer_iterations
         else:

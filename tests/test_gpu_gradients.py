@@ -110,7 +110,12 @@ def test_adjoint_gradient_matches_central_differences_3d(mixed):
         vals = [_c1212(mu * (1 + sgn * h * d), prob) for sgn in (1.0, -1.0)]
         fd = (vals[0] - vals[1]) / (2 * h)
         an = float((m.grad * mu * d).sum())
-        assert abs(fd - an) <= 1e-6 * abs(an) + 1e-10, (fd, an)
+        # the mean stress is linear in the solver's residual: each solve carries
+        # ~tol of noise, which the difference divides by 2h (~1e-6 relative
+        # here); the Krylov path varies between the perturbed solves, the FP64
+        # basic scheme does not
+        rtol = 1e-5 if mixed else 1e-6
+        assert abs(fd - an) <= rtol * abs(an) + 1e-10, (fd, an)
 
 
 @pytest.mark.gpu
