@@ -44,6 +44,9 @@ extern "C" {
 
 #define JB_TRUNCATED 0
 #define JB_FILTERED 1
+/* FiniteDifferences2D/3D, janus.green.willot2015 (janus/green.pyx:976-1036):
+ * Gamma0 at k_i = sin(phi_i) prod_{j != i} cos(phi_j), phi_i = pi b_i / n_i */
+#define JB_WILLOT 2
 
 typedef struct jb_fft_s jb_fft;
 typedef struct jb_green_s jb_green;
@@ -100,9 +103,10 @@ int jb_isotropic_apply(int dim, double sph, double dev, const double *x,
 
 /* ---- discrete Green operators ----------------------------------------- */
 
-/* Replaces janus.green.truncated / filtered (janus/green.pyx:22-36) and the
- * TruncatedGreenOperator2D/3D, FilteredGreenOperator2D/3D constructors
- * (100-141, 261-307, 428-430, 501-503, 593-605, 708-728). */
+/* Replaces janus.green.truncated / filtered / willot2015 (janus/green.pyx:
+ * 22-36, 1030-1036) and the TruncatedGreenOperator2D/3D,
+ * FilteredGreenOperator2D/3D, FiniteDifferences2D/3D constructors (100-141,
+ * 261-307, 428-430, 501-503, 593-605, 708-728, 976-1027). */
 int jb_green_create(int dim, const int64_t *shape, double h, double g,
                     double nu, int variant, int dtype, jb_green **out);
 int jb_green_destroy(jb_green *green);

@@ -20,6 +20,7 @@ JB_F64 = 0
 JB_F32 = 1
 JB_TRUNCATED = 0
 JB_FILTERED = 1
+JB_WILLOT = 2
 
 _lock = threading.Lock()
 _lib = None

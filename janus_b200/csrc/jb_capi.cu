@@ -591,8 +591,8 @@ int jb_green_create(int dim, const int64_t* shape, double h, double g, double nu
   *out = nullptr;
   JB_TRY(check_shape(dim, shape, dtype));
   if (!(h > 0.)) return fail(JB_EINVAL, "h must be > 0 (was " + std::to_string(h) + ")");
-  if (variant != JB_TRUNCATED && variant != JB_FILTERED)
-    return fail(JB_EINVAL, "variant must be JB_TRUNCATED or JB_FILTERED");
+  if (variant != JB_TRUNCATED && variant != JB_FILTERED && variant != JB_WILLOT)
+    return fail(JB_EINVAL, "variant must be JB_TRUNCATED, JB_FILTERED or JB_WILLOT");
   jb_green* G = new jb_green();
   G->dim = dim;
   G->dtype = dtype;
@@ -625,6 +625,17 @@ int jb_green_create(int dim, const int64_t* shape, double h, double g, double nu
       std::vector<double> kt(n);
       for (int64_t b = 0; b < n; ++b) kt[b] = 2 * b > n ? sd * (b - n) : sd * b;
       int r = upload_table(G, dtype, kt, &G->gt.kt[d]);
+      if (r != JB_OK) return cleanup(r);
+    } else if (variant == JB_WILLOT) {
+      // sin and cos of phi = 0.5 * s * h * b (green.pyx:983-989, 1001-1013)
+      std::vector<double> sn(n), cs(n);
+      for (int64_t b = 0; b < n; ++b) {
+        const double phi = 0.5 * sd * h * (double)b;
+        sn[b] = sin(phi);
+        cs[b] = cos(phi);
+      }
+      int r = upload_table(G, dtype, sn, &G->gt.kn[d]);
+      if (r == JB_OK) r = upload_table(G, dtype, cs, &G->gt.kp[d]);
       if (r != JB_OK) return cleanup(r);
     } else {
       std::vector<double> kn(n), kp(n), wn(n), wp(n);
@@ -721,6 +732,25 @@ int jb_green_matrix(jb_green* G, const int32_t* b, double* out) {
     for (int d = 0; d < dim; ++d) {
       const int64_t n = G->n[d];
       k[d] = 2 * (int64_t)b[d] > n ? G->s[d] * (b[d] - n) : G->s[d] * b[d];
+    }
+    green_matrix_dim(dim, aux, k, out);
+    return JB_OK;
+  }
+  if (G->variant == JB_WILLOT) {
+    // green.pyx:983-989 (2D), 1001-1016 (3D), products left to right
+    double c[3], sn[3], k[3];
+    for (int d = 0; d < dim; ++d) {
+      const double phi = 0.5 * G->s[d] * G->h * b[d];
+      c[d] = cos(phi);
+      sn[d] = sin(phi);
+    }
+    if (dim == 2) {
+      k[0] = sn[0] * c[1];
+      k[1] = c[0] * sn[1];
+    } else {
+      k[0] = sn[0] * c[1] * c[2];
+      k[1] = c[0] * sn[1] * c[2];
+      k[2] = c[0] * c[1] * sn[2];
     }
     green_matrix_dim(dim, aux, k, out);
     return JB_OK;

@@ -37,13 +37,31 @@ template <typename T> struct GreenTables {
   const T* wp[3];
   T inv2g;  // 1 / (2 g)
   T c1;     // 1 / (1 - nu)
-  int variant;  // 0 truncated, 1 filtered
+  int variant;  // 0 truncated, 1 filtered, 2 finite differences (Willot)
 };
+
+// Gamma(k) depends on k / |k| only.  In FP32 the rank-4 terms form k^4 and
+// 1/|k|^4, which underflow / overflow for tiny k (the finite-difference
+// wave-vector has components ~1e-17 where two cosines vanish): scale k by
+// its largest component first.  FP64 keeps the reference's arithmetic.
+template <typename T>
+__device__ __forceinline__ void scale_k(T& k0, T& k1, T& k2) {
+  if constexpr (sizeof(T) == 4) {
+    const T m = fmaxf(fabsf(k0), fmaxf(fabsf(k1), fabsf(k2)));
+    if (m > T(0)) {
+      const T inv = T(1) / m;
+      k0 *= inv;
+      k1 *= inv;
+      k2 *= inv;
+    }
+  }
+}
 
 // acc += w * Gamma(k) : t  (3D, Mandel, real and imaginary parts)
 template <typename T, typename C>
 __device__ __forceinline__ void gamma3_acc(T k0, T k1, T k2, T w, const C* t, C* acc,
                                            T inv2g, T c1) {
+  scale_k(k0, k1, k2);
   const T kk = k0 * k0 + k1 * k1 + k2 * k2;
   if (kk == T(0)) return;
   const T q = rcp_rn(kk);
@@ -83,6 +101,8 @@ __device__ __forceinline__ void gamma3_acc(T k0, T k1, T k2, T w, const C* t, C*
 template <typename T, typename C>
 __device__ __forceinline__ void gamma2_acc(T k0, T k1, T w, const C* t, C* acc, T inv2g,
                                            T c1) {
+  T kz = T(0);
+  scale_k(k0, k1, kz);
   const T kk = k0 * k0 + k1 * k1;
   if (kk == T(0)) return;
   const T q = rcp_rn(kk);
@@ -291,8 +311,25 @@ __device__ __forceinline__ void mn_accumulate2(T k0, T k1, T al, T be, T* mn) {
   mn[7] += b11 * p11;
 }
 
+// finite-difference wave-vector from per-axis (sin, cos) of phi = pi b / n
+// (green.pyx:983-989, 1001-1016): k_i = sin(phi_i) prod_{j != i} cos(phi_j),
+// products left to right as in the reference
+template <int DIM, typename T>
+__device__ __forceinline__ void willot_k(const T* a0, const T* a1, const T* a2, T& k0, T& k1,
+                                         T& k2) {
+  if (DIM == 2) {
+    k0 = a0[0] * a1[1];
+    k1 = a0[1] * a1[0];
+    k2 = T(0);
+  } else {
+    k0 = a0[0] * a1[1] * a2[1];
+    k1 = a0[1] * a1[0] * a2[1];
+    k2 = a0[1] * a1[1] * a2[0];
+  }
+}
+
 // M/N of one coefficient from its per-axis values (AxisK: truncated k in
-// v[0]; filtered k-, k+, w-, w+)
+// v[0]; filtered k-, k+, w-, w+; finite differences sin, cos)
 template <int DIM, typename T>
 __device__ __forceinline__ void mn_build(int variant, const T* a0, const T* a1, const T* a2,
                                          T inv2g, T c1, T* mn) {
@@ -300,13 +337,16 @@ __device__ __forceinline__ void mn_build(int variant, const T* a0, const T* a1, 
 #pragma unroll
   for (int i = 0; i < NT; ++i) mn[i] = T(0);
   constexpr int NA = DIM == 3 ? 8 : 4;
-  const int na = variant == 0 ? 1 : NA;
+  const int na = variant == 1 ? NA : 1;
   for (int a = 0; a < na; ++a) {
     T k0, k1, k2 = T(0), w;
     if (variant == 0) {
       k0 = a0[0];
       k1 = a1[0];
       if (DIM == 3) k2 = a2[0];
+      w = T(1);
+    } else if (variant == 2) {
+      willot_k<DIM, T>(a0, a1, a2, k0, k1, k2);
       w = T(1);
     } else if (DIM == 3) {
       const int s0 = a >> 2, s1 = (a >> 1) & 1, s2 = a & 1;
@@ -320,6 +360,7 @@ __device__ __forceinline__ void mn_build(int variant, const T* a0, const T* a1, 
       k1 = a1[s1];
       w = a0[2 + s0] * a1[2 + s1];
     }
+    scale_k(k0, k1, k2);
     const T kk = k0 * k0 + k1 * k1 + k2 * k2;
     if (kk == T(0)) continue;
     const T q = rcp_rn(kk);
@@ -406,6 +447,10 @@ __device__ __forceinline__ AxisK<T> axis_values(const GreenTables<T>& g, int d, 
   if (g.variant == 0) {
     r.v[0] = g.kt[d][bd];
     r.v[1] = r.v[2] = r.v[3] = T(0);
+  } else if (g.variant == 2) {
+    r.v[0] = g.kn[d][bd];  // sin(phi)
+    r.v[1] = g.kp[d][bd];  // cos(phi)
+    r.v[2] = r.v[3] = T(0);
   } else {
     r.v[0] = g.kn[d][bd];
     r.v[1] = g.kp[d][bd];
@@ -425,14 +470,16 @@ __device__ __forceinline__ void green_contract_k(int variant, const AxisK<T>& a0
   C t[S];
 #pragma unroll
   for (int i = 0; i < S; ++i) t[i] = te[i];
-  if (variant == 0) {
+  if (variant == 0 || variant == 2) {
     C acc[S];
 #pragma unroll
     for (int i = 0; i < S; ++i) acc[i] = mkc(T(0), T(0));
+    T k0 = a0.v[0], k1 = a1.v[0], k2 = a2.v[0];
+    if (variant == 2) willot_k<DIM, T>(a0.v, a1.v, a2.v, k0, k1, k2);
     if (DIM == 2)
-      gamma2_acc(a0.v[0], a1.v[0], T(1), t, acc, inv2g, c1);
+      gamma2_acc(k0, k1, T(1), t, acc, inv2g, c1);
     else
-      gamma3_acc(a0.v[0], a1.v[0], a2.v[0], T(1), t, acc, inv2g, c1);
+      gamma3_acc(k0, k1, k2, T(1), t, acc, inv2g, c1);
 #pragma unroll
     for (int i = 0; i < S; ++i) te[i] = acc[i];
   } else {

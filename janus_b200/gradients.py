@@ -38,12 +38,12 @@ import torch
 
 from . import _arrays as A
 from . import _lib
-from .green import filtered, truncated
+from .green import filtered, truncated, willot2015
 from .material.elastic.linear import isotropic as material
 from .operators import LocalPhaseOperator
 from .solvers import BasicScheme, MixedScheme
 
-_FACTORY = {"truncated": truncated, "filtered": filtered}
+_FACTORY = {"truncated": truncated, "filtered": filtered, "willot": willot2015}
 
 
 def bulk_factor(nu, dim):
@@ -60,7 +60,7 @@ class StiffnessFieldProblem:
     Poisson ratio ``nu``, loaded by the rows of ``avg_eps``.
 
     mu0, nu0: reference medium (default: mid-range of the field, nu).
-    variant: "truncated" or "filtered" Green operator; h: voxel size.
+    variant: "truncated", "filtered" or "willot" Green operator; h: voxel size.
     mixed: FP32 bulk iterations with FP64 defect correction (else plain
     FP64), the correction solved by ``inner_method`` ("bicgstab": ``inner``
     BiCGSTAB iterations; "basic": ``inner - 1`` basic iterations); tol:
@@ -109,7 +109,7 @@ class _Cell:
         self.local = LocalPhaseOperator(self.dim, self.shape, None, sph.flatten(),
                                         dev.flatten(), torch.float64)
         if prob.variant not in _FACTORY:
-            raise ValueError("variant must be 'truncated' or 'filtered'")
+            raise ValueError("variant must be 'truncated', 'filtered' or 'willot'")
         self.green = _FACTORY[prob.variant](self.mat0.green_operator(), self.shape, prob.h)
         self.prob = prob
 

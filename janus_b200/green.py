@@ -1,9 +1,10 @@
 """Discrete Green operators for strains (the ``janus.green`` module).
 
-Mirrors janus/green.pyx:22-973 for the truncated and filtered
-discretisations, 2D and 3D:
+Mirrors janus/green.pyx:22-1036 for the truncated, filtered and
+finite-difference (Willot 2015) discretisations, 2D and 3D:
 
-* ``truncated(green, n, h, transform=None)`` / ``filtered(...)`` (22-36);
+* ``truncated(green, n, h, transform=None)`` / ``filtered(...)`` (22-36),
+  ``willot2015(...)`` (1030-1036);
 * ``set_frequency(b)`` with the reference's range checks (146-163,
   312-334), ``to_memoryview(out)`` (165-171, 336-342), ``apply_by_freq(tau,
   eta)`` (173-180, 344-351): per-index host calls evaluated by the native
@@ -48,6 +49,17 @@ def filtered(green, n, h, transform=None, dtype=None):
         return FilteredGreenOperator2D(green, n, h, transform, dtype)
     elif green.dim == 3:
         return FilteredGreenOperator3D(green, n, h, transform, dtype)
+    raise ValueError('dim must be 2 or 3 (was {0})'.format(green.dim))
+
+
+def willot2015(green, n, h, transform=None, dtype=None):
+    """Finite-difference ("rotated scheme", Willot 2015) discrete Green
+    operator (green.pyx:1030-1036): Gamma0 at the modified wave-vector
+    k_i = sin(phi_i) prod_{j != i} cos(phi_j), phi_i = pi b_i / n_i."""
+    if green.dim == 2:
+        return FiniteDifferences2D(green, n, h, transform, dtype)
+    elif green.dim == 3:
+        return FiniteDifferences3D(green, n, h, transform, dtype)
     raise ValueError('dim must be 2 or 3 (was {0})'.format(green.dim))
 
 
@@ -212,3 +224,13 @@ class FilteredGreenOperator2D(DiscreteGreenOperator2D):
 class FilteredGreenOperator3D(DiscreteGreenOperator3D):
     """green.pyx:697-973"""
     _variant = _lib.JB_FILTERED
+
+
+class FiniteDifferences2D(DiscreteGreenOperator2D):
+    """green.pyx:976-992"""
+    _variant = _lib.JB_WILLOT
+
+
+class FiniteDifferences3D(DiscreteGreenOperator3D):
+    """green.pyx:995-1027"""
+    _variant = _lib.JB_WILLOT

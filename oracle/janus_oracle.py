@@ -155,6 +155,24 @@ def filtered_matrix(b, n, h, g, nu) -> np.ndarray:
     return acc
 
 
+def willot_wavevector(b, n, h: float) -> np.ndarray:
+    """k(b) of FiniteDifferences{2,3}D.c_set_frequency (green.pyx:983-989,
+    1001-1016): phi_i = 0.5*s_i*h*b_i (b_i not wrapped), k_0 = sin(phi_0)
+    cos(phi_1) [cos(phi_2)], k_1 = cos(phi_0) sin(phi_1) [cos(phi_2)],
+    k_2 = cos(phi_0) cos(phi_1) sin(phi_2); products left to right."""
+    dim = len(n)
+    phi = [0.5 * (2. * math.pi / (h * ni)) * h * bi for bi, ni in zip(b, n)]
+    c = [math.cos(v) for v in phi]
+    sn = [math.sin(v) for v in phi]
+    if dim == 2:
+        return np.array([sn[0] * c[1], c[0] * sn[1]])
+    return np.array([sn[0] * c[1] * c[2], c[0] * sn[1] * c[2], c[0] * c[1] * sn[2]])
+
+
+def willot_matrix(b, n, h, g, nu) -> np.ndarray:
+    return green_matrix(willot_wavevector(b, n, h), g, nu)
+
+
 def _half_spectrum_k(n, h):
     """Per-axis truncated wave-numbers on the r2c half spectrum."""
     ks = []
@@ -225,12 +243,27 @@ def spectral_green_field(n, h, g, nu, variant="truncated") -> np.ndarray:
     """Gamma-hat on the r2c half spectrum, shape (n0, [n1,] n_last//2+1, s, s).
 
     truncated: the k-map of green.pyx:464-481 / 542-566 (Nyquist -> +pi/h);
-    filtered: the 2^d-alias weighted sum of green.pyx:609-670 / 732-910.
+    filtered: the 2^d-alias weighted sum of green.pyx:609-670 / 732-910;
+    willot: the finite-difference wave-vector of green.pyx:976-1036.
     """
     dim = len(n)
     if variant == "truncated":
         kgrid = np.meshgrid(*_half_spectrum_k(n, h), indexing="ij")
         return _green_field(kgrid, g, nu)
+    if variant == "willot":
+        cs, sn = [], []
+        for i, ni in enumerate(n):
+            nb = ni if i < dim - 1 else ni // 2 + 1
+            phi = 0.5 * (2. * np.pi / (h * ni)) * h * np.arange(nb)
+            cs.append(np.cos(phi))
+            sn.append(np.sin(phi))
+        if dim == 2:
+            C0, C1 = np.meshgrid(cs[0], cs[1], indexing="ij")
+            S0, S1 = np.meshgrid(sn[0], sn[1], indexing="ij")
+            return _green_field([S0 * C1, C0 * S1], g, nu)
+        C0, C1, C2 = np.meshgrid(*cs, indexing="ij")
+        S0, S1, S2 = np.meshgrid(*sn, indexing="ij")
+        return _green_field([S0 * C1 * C2, C0 * S1 * C2, C0 * C1 * S2], g, nu)
     acc = None
     s = [2. * np.pi / (h * ni) for ni in n]
     axes = []

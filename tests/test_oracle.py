@@ -86,8 +86,13 @@ def test_oracle_tutorial_known_answer():
 GRID_SIZES = [(8, 8), (8, 16), (16, 8), (4, 4, 4), (4, 8, 16), (16, 8, 4)]
 
 
+_REF_FACTORY = {"truncated": "truncated", "filtered": "filtered", "willot": "willot2015"}
+_ORACLE_MATRIX = {"truncated": O.truncated_matrix, "filtered": O.filtered_matrix,
+                  "willot": O.willot_matrix}
+
+
 @pytest.mark.parametrize("n", GRID_SIZES)
-@pytest.mark.parametrize("variant", ["truncated", "filtered"])
+@pytest.mark.parametrize("variant", ["truncated", "filtered", "willot"])
 def test_oracle_matrices_match_reference_build(n, variant):
     ref = reference_checker()
     if ref is None:
@@ -96,15 +101,15 @@ def test_oracle_matrices_match_reference_build(n, variant):
     import janus.material.elastic.linear.isotropic as rmat
     dim = len(n)
     g = rmat.create(0.75, 0.3, dim).green_operator()
-    op = (rgreen.truncated if variant == "truncated" else rgreen.filtered)(g, n, 1.0)
-    mat = O.truncated_matrix if variant == "truncated" else O.filtered_matrix
+    op = getattr(rgreen, _REF_FACTORY[variant])(g, n, 1.0)
+    mat = _ORACLE_MATRIX[variant]
     for b in itertools.product(*[range(v) for v in n]):
         op.set_frequency(np.asarray(b, dtype=np.intc))
         np.testing.assert_array_equal(np.asarray(op.to_memoryview()),
                                       mat(b, n, 1.0, 0.75, 0.3))
 
 
-@pytest.mark.parametrize("variant", ["truncated", "filtered"])
+@pytest.mark.parametrize("variant", ["truncated", "filtered", "willot"])
 @pytest.mark.parametrize("shape", [(12, 10), (6, 5, 8)])
 def test_oracle_basic_scheme_matches_reference_build(variant, shape):
     ref = reference_checker()
@@ -132,7 +137,7 @@ def test_oracle_basic_scheme_matches_reference_build(variant, shape):
     for idx in np.ndindex(*shape):
         ops[idx] = tens[phase[idx]]
     loc = rops.block_diagonal_operator(ops)
-    gr = (rgreen.truncated if variant == "truncated" else rgreen.filtered)(
+    gr = getattr(rgreen, _REF_FACTORY[variant])(
         rmat.create(g0, nu0, dim).green_operator(), shape, 1.0, rfft.create_real(shape))
     eps = np.empty(shape + (s,))
     eps[...] = E
