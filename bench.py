@@ -422,7 +422,7 @@ def run_gpu(args, rank, world, dist):
             # the same defect correction with a Krylov inner solver (BiCGSTAB
             # on the basic scheme's operator, FP32)
             kry = MixedScheme(green, loc, nload=6, inner=args.krylov_inner, method="bicgstab")
-            kry.run(E, tol=1e-3, max_outer=1)  # warm
+            kry.run(E, tol=1e-30, max_outer=2)  # warm: one correction allocates the Krylov fields
             torch.cuda.synchronize()
             a.record()
             rk = kry.run(E, tol=args.tol, max_outer=args.solve_max_iter)
@@ -629,7 +629,7 @@ def run_voronoi(args, rank):
         }
         del mixed
         kry = MixedScheme(green, loc, nload=len(E), inner=args.krylov_inner, method="bicgstab")
-        kry.run(E, tol=1e-2, max_outer=1)  # warm
+        kry.run(E, tol=1e-30, max_outer=2)  # warm: one correction allocates the Krylov fields
         torch.cuda.synchronize()
         a.record()
         rk = kry.run(E, tol=args.tol, max_outer=args.solve_max_iter)
