@@ -165,6 +165,15 @@ int jb_green_apply_by_freq_device(jb_green *green, int64_t count,
 int jb_local_create(int dim, const int64_t *shape, int nphase,
                     const double *sph, const double *dev, const void *phase,
                     int index_bytes, int dtype, jb_local **out);
+/* BlockDiagonalOperator2D/3D over general linear local operators
+ * (LinearOperator, FourthRankCubicTensor2D: janus/operators.pyx:195-254,
+ * 411-450): one row-major s x s matrix (C - C0 of the phase) per table entry,
+ * mats host double[nphase][s][s]; phase / index_bytes as jb_local_create.
+ * Applied as y_i = sum_j m_ij x_j in j order without FMA contraction (the
+ * reference's c_apply order). */
+int jb_local_create_matrix(int dim, const int64_t *shape, int nphase,
+                           const double *mats, const void *phase,
+                           int index_bytes, int dtype, jb_local **out);
 int jb_local_destroy(jb_local *local);
 /* BlockDiagonalOperator2D/3D.c_apply (657-664, 708-716), bitwise the
  * reference arithmetic; x == y allowed. */

@@ -59,6 +59,8 @@ _SIGS = {
                                        c_void_p], c_int),
     "jb_local_create": ([c_int, P_int64, c_int, P_double, P_double, c_void_p, c_int, c_int,
                          ctypes.POINTER(c_void_p)], c_int),
+    "jb_local_create_matrix": ([c_int, P_int64, c_int, P_double, c_void_p, c_int, c_int,
+                                ctypes.POINTER(c_void_p)], c_int),
     "jb_local_destroy": ([c_void_p], c_int),
     "jb_local_apply": ([c_void_p, c_void_p, c_void_p, c_int64, c_void_p], c_int),
     "jb_block_linear_apply": ([c_int, c_int64, c_int, c_int, c_void_p, c_void_p, c_void_p,

@@ -260,7 +260,7 @@ struct jb_green_s {
 };
 
 struct jb_local_s {
-  int dim = 0, dtype = 0, nphase = 0, index_bytes = 1;
+  int dim = 0, dtype = 0, nphase = 0, index_bytes = 1, kind = 0;
   int64_t n[3] = {1, 1, 1};
   int64_t nvox = 0;
   void* phase = nullptr;
@@ -882,6 +882,65 @@ int jb_local_create(int dim, const int64_t* shape, int nphase, const double* sph
   return JB_OK;
 }
 
+int jb_local_create_matrix(int dim, const int64_t* shape, int nphase, const double* mats,
+                           const void* phase, int index_bytes, int dtype, jb_local** out) {
+  if (!out) return fail(JB_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  if (dim != 2 && dim != 3) return fail(JB_EINVAL, "dim must be 2 or 3");
+  if (dtype != F64 && dtype != F32) return fail(JB_EINVAL, "dtype must be JB_F64 or JB_F32");
+  if (nphase < 1) return fail(JB_EINVAL, "nphase must be >= 1");
+  if (index_bytes != 0 && index_bytes != 1 && index_bytes != 4)
+    return fail(JB_EINVAL, "index_bytes must be 0 (per-voxel field), 1 or 4");
+  if (index_bytes == 1 && nphase > 256) return fail(JB_EINVAL, "uint8 phase map allows 256 phases");
+  if (!mats || (index_bytes != 0 && !phase)) return fail(JB_EINVAL, "NULL argument");
+  jb_local* L = new jb_local();
+  L->dim = dim;
+  L->dtype = dtype;
+  L->nphase = nphase;
+  L->index_bytes = index_bytes;
+  L->kind = 1;
+  L->nvox = 1;
+  for (int d = 0; d < dim; ++d) {
+    if (shape[d] <= 0) {
+      delete L;
+      return fail(JB_EINVAL, "shape must be > 0");
+    }
+    L->n[d] = shape[d];
+    L->nvox *= shape[d];
+  }
+  if (index_bytes == 0 && (int64_t)nphase != L->nvox) {
+    delete L;
+    return fail(JB_EINVAL, "a per-voxel field needs nphase equal to the voxel count");
+  }
+  const int S = dim == 2 ? 3 : 6;
+  const size_t count = (size_t)nphase * S * S;
+  const size_t rs = real_size(dtype);
+  int r = dev_alloc(&L->table, count * rs);
+  if (r == JB_OK && index_bytes != 0) r = dev_alloc(&L->phase, (size_t)L->nvox * index_bytes);
+  if (r != JB_OK) {
+    if (L->table) cudaFree(L->table);
+    delete L;
+    return r;
+  }
+  cudaError_t e;
+  if (dtype == F64) {
+    e = cudaMemcpy(L->table, mats, count * 8, cudaMemcpyHostToDevice);
+  } else {
+    std::vector<float> f(mats, mats + count);
+    e = cudaMemcpy(L->table, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && index_bytes != 0)
+    e = cudaMemcpy(L->phase, phase, (size_t)L->nvox * index_bytes, cudaMemcpyDefault);
+  if (e != cudaSuccess) {
+    cudaFree(L->table);
+    cudaFree(L->phase);
+    delete L;
+    return fail(JB_ECUDA, std::string("jb_local_create_matrix: ") + cudaGetErrorString(e));
+  }
+  *out = L;
+  return JB_OK;
+}
+
 int jb_local_destroy(jb_local* L) {
   if (!L) return JB_OK;
   cudaFree(L->table);
@@ -897,6 +956,7 @@ static jb::LocalDesc local_desc(const jb_local* L) {
   d.table = L->table;
   d.nphase = L->nphase;
   d.dim = L->dim;
+  d.kind = L->kind;
   return d;
 }
 

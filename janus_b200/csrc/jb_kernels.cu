@@ -68,6 +68,35 @@ __device__ __forceinline__ void iso_apply(T* p, T tr, T dev, int dim) {
   }
 }
 
+// y = M x for one voxel, M row-major s x s: y_i = (((0 + m_i0 x_0) + m_i1 x_1)
+// + ...) without FMA contraction, the order of LinearOperator.c_apply and of
+// FourthRankCubicTensor2D.c_apply (janus/operators.pyx:209-214, 435-441)
+template <typename T>
+__device__ __forceinline__ void mat_apply(T* p, const T* m, int C) {
+  T x[6];
+  for (int c = 0; c < C; ++c) x[c] = p[c];
+  for (int i = 0; i < C; ++i) {
+    T y = mul_rn(m[i * C], x[0]);
+    for (int j = 1; j < C; ++j) y = add_rn(y, mul_rn(m[i * C + j], x[j]));
+    p[i] = y;
+  }
+}
+
+// the local operator of entry ph: isotropic (tr, dev) or a full matrix
+template <typename T>
+__device__ __forceinline__ void local_apply(T* p, const T* tab, int ph, int kind, int dim) {
+  const int C = dim == 2 ? 3 : 6;
+  if (kind == 0)
+    iso_apply<T>(p, tab[2 * ph], tab[2 * ph + 1], dim);
+  else
+    mat_apply<T>(p, tab + (size_t)ph * C * C, C);
+}
+
+// reals per table entry of a local operator
+__host__ __device__ __forceinline__ int local_entry(int kind, int dim) {
+  return kind == 0 ? 2 : (dim == 2 ? 9 : 36);
+}
+
 // phase id of voxel v: uint8 or int32 map; index_bytes 0 = one table entry
 // per voxel (stiffness fields)
 __device__ __forceinline__ int load_phase(const void* phase, int ib, int64_t v) {
@@ -125,7 +154,8 @@ template <typename T> struct RowsArgs {
   const void* phase;
   int index_bytes;
   const T* table;
-  int nphase;  // table entries (staged in shared memory when <= kTabStage)
+  int nphase;  // table entries (staged in shared memory when <= kTabStage reals / 2)
+  int kind;    // local operator entries: 0 (tr, dev), 1 s x s matrices
   int dim;
   const double* E;
   double* partials;
@@ -270,8 +300,9 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   if constexpr (LOCAL) {
     for (int i = threadIdx.x; i < rows_here * n; i += blockDim.x)
       phs[i] = load_phase(a.phase, a.index_bytes, row0 * n + i);
-    if (a.nphase <= kTabStage) {
-      for (int i = threadIdx.x; i < 2 * a.nphase; i += blockDim.x) tabs[i] = a.table[i];
+    const int tabn = a.nphase * local_entry(a.kind, a.dim);
+    if (tabn <= 2 * kTabStage) {
+      for (int i = threadIdx.x; i < tabn; i += blockDim.x) tabs[i] = a.table[i];
       tab = tabs;
     }
   }
@@ -287,10 +318,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       T x[kC];
       if (rr < rows_here) {
         load_voxel<T, kC>(Br + rr * ldb + e * kC, x);
-        if constexpr (LOCAL) {
-          const int ph = phs[rr * n + e];
-          iso_apply<T>(x, tab[2 * ph], tab[2 * ph + 1], kC == 3 ? 2 : 3);
-        }
+        if constexpr (LOCAL) local_apply<T>(x, tab, phs[rr * n + e], a.kind, kC == 3 ? 2 : 3);
       } else {
 #pragma unroll
         for (int c = 0; c < kC; ++c) x[c] = T(0);
@@ -304,10 +332,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
         if (rr < rows_here) {
 #pragma unroll
           for (int c = 0; c < kC; ++c) v[c] = Br[rr * ldb + e * kC + c];
-          if constexpr (LOCAL) {
-            const int ph = phs[rr * n + e];
-            iso_apply<T>(v, tab[2 * ph], tab[2 * ph + 1], kC == 3 ? 2 : 3);
-          }
+          if constexpr (LOCAL) local_apply<T>(v, tab, phs[rr * n + e], a.kind, kC == 3 ? 2 : 3);
         } else {
 #pragma unroll
           for (int c = 0; c < kC; ++c) v[c] = T(0);
@@ -875,7 +900,7 @@ __global__ void local_kernel(LocalDesc loc, const T* table, int C, int L, int64_
     const int ph = load_phase(loc.phase, loc.index_bytes, v);
     T p[6];
     for (int c = 0; c < C; ++c) p[c] = x[i * C + c];
-    iso_apply<T>(p, table[2 * ph], table[2 * ph + 1], loc.dim);
+    local_apply<T>(p, table, ph, loc.kind, loc.dim);
     for (int c = 0; c < C; ++c) y[i * C + c] = p[c];
   }
 }
@@ -892,7 +917,7 @@ __global__ void local_sum_kernel(LocalDesc loc, const T* table, int C, int64_t n
     const int ph = load_phase(loc.phase, loc.index_bytes, v);
     T p[6];
     for (int c = 0; c < C; ++c) p[c] = el[v * C + c];
-    iso_apply<T>(p, table[2 * ph], table[2 * ph + 1], loc.dim);
+    local_apply<T>(p, table, ph, loc.kind, loc.dim);
     for (int c = 0; c < C; ++c) acc[c] += static_cast<double>(p[c]);
   }
   for (int c = 0; c < C; ++c) {
@@ -1096,24 +1121,27 @@ int tile_threads(int W) {
 // local operator, the tile's phase ids and the staged phase table.  This is
 // the kernels' exact layout (each region aligned to 16 bytes): three CTAs
 // per SM of the FP64 c2r update kernel at n = 128 fit with 96 bytes to spare.
-size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local, int nphase) {
+size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local, int nphase,
+                 int entry = 2) {
   const size_t cs = dtype == F64 ? 16 : 8;
-  const size_t staged = nphase <= kTabStage ? (size_t)nphase : 0;
+  // staged table reals (2 * kTabStage at most)
+  const size_t treal = (size_t)nphase * entry;
+  const size_t staged = treal <= 2 * (size_t)kTabStage ? treal : 0;
   auto a16 = [](size_t v) { return (v + 15) / 16 * 16; };
   size_t off = a16(n * cs) + (size_t)(n + 2) * w * cs;  // twiddles | A
   off = a16(off) + (size_t)(n + 2) * w * cs;           // B
   if (update) off = a16(off) + (size_t)r * n * C * (cs / 2) + (size_t)(r - 1) * 32;
-  if (local) off = a16(off + (size_t)r * n * 4) + 2 * staged * (cs / 2);
+  if (local) off = a16(off + (size_t)r * n * 4) + staged * (cs / 2);
   return off;
 }
 
 bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem,
-                bool local = false, int nphase = 0) {
+                bool local = false, int nphase = 0, int entry = 2) {
   const size_t cs = dtype == F64 ? 16 : 8;
   int r = (24 + C - 1) / C;
   for (;;) {
     const int w = (r * C + 1) / 2;
-    const size_t bytes = rows_smem(dtype, n, C, r, w, update, local, nphase);
+    const size_t bytes = rows_smem(dtype, n, C, r, w, update, local, nphase, entry);
     if (bytes <= kSmemBudget || r == 1) {
       if (bytes > kSmemCap - 4096) return false;
       *R = r;
@@ -1326,8 +1354,9 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   if (C != 1 && C != 3 && C != 6) return cudaErrorInvalidValue;
   if (local && C == 1) return cudaErrorInvalidValue;
   const int nphase = local ? local->nphase : 0;
+  const int entry = local ? local_entry(local->kind, local->dim) : 2;
   if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem, local != nullptr,
-                  nphase))
+                  nphase, entry))
     return cudaErrorInvalidValue;
   a.x = static_cast<const T*>(x);
   a.out = static_cast<cx<T>*>(out);
@@ -1345,6 +1374,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     a.index_bytes = local->index_bytes;
     a.table = static_cast<const T*>(local->table);
     a.nphase = local->nphase;
+    a.kind = local->kind;
     a.dim = local->dim;
   }
   if ((n == 64 || n == 128 || n == 256) && (C == 3 || C == 6)) {
@@ -1352,7 +1382,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     const int wct = n <= 128 ? 12 : 6;
     const int rct = 2 * wct / C;
     const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, false,
-                                 local != nullptr, nphase);
+                                 local != nullptr, nphase, entry);
     if (sct <= kSmemBudget + 24 * 1024) {
       RowsArgs<T> b = a;
       b.R = rct;

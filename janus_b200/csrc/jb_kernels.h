@@ -42,11 +42,12 @@ struct RealGeom {
 // Local operator (C - C0):eps on a phase map; table holds (tr, dev) pairs
 // in the field's precision.
 struct LocalDesc {
-  const void* phase = nullptr;  // uint8 or int32 per voxel, row-major grid
-  int index_bytes = 1;          // 1 or 4
-  const void* table = nullptr;  // device, T[2 * nphase]
+  const void* phase = nullptr;  // uint8 or int32 per voxel, row-major grid (index_bytes 0: none)
+  int index_bytes = 1;          // 0 (one entry per voxel), 1 or 4
+  const void* table = nullptr;  // device: kind 0 T[nphase][2] = (tr, dev); kind 1 T[nphase][s][s]
   int nphase = 1;
   int dim = 2;
+  int kind = 0;                 // 0 isotropic (tr, dev), 1 full s x s matrix per entry
 };
 
 // Solver epilogue of the last pass (y = scale * c2r(spectrum)):

@@ -5,7 +5,8 @@ Mirrors ``janus.operators`` (janus/operators.pyx:53-890) for the hot path:
 * ``AbstractOperator`` / ``AbstractLinearOperator`` with ``init_sizes``,
   ``apply`` and ``to_memoryview`` (113-192);
 * ``isotropic_4(sph, dev, dim)`` and ``FourthRankIsotropicTensor{2,3}D``
-  (53-67, 257-408);
+  (53-67, 257-408); ``LinearOperator(a)`` (195-254) and
+  ``FourthRankCubicTensor2D(t1111, t1122, t1212, theta)`` (411-450);
 * ``AbstractStructuredOperator{2,3}D`` with ``init_shapes`` and ``apply``
   (452-614);
 * ``block_diagonal_operator(loc)`` / ``BlockDiagonalOperator{2,3}D(loc)``
@@ -15,8 +16,10 @@ Mirrors ``janus.operators`` (janus/operators.pyx:53-890) for the hot path:
 
 Field-wide operators run in the native library; a ``BlockDiagonalOperator``
 built from isotropic tensors becomes a phase map (one index per voxel) plus
-a table of (tr, dev) coefficients, applied with the reference's arithmetic
-(bitwise identical results).  Single-vector ``apply`` calls of the local
+a table of (tr, dev) coefficients, one built from other square linear local
+operators (cubic tensors, ``LinearOperator``) a phase map plus a table of
+their matrices; both are applied with the reference's arithmetic (bitwise
+identical results) and both drive the solvers.  Single-vector ``apply`` calls of the local
 tensors run in the library's host code with the reference's operation order.
 
 Difference from the reference: block-diagonal operators copy ``loc`` / ``a``
@@ -26,6 +29,7 @@ to the device when they are built (the reference keeps a shallow reference);
 from __future__ import annotations
 
 import ctypes
+import math
 
 import numpy as np
 import torch
@@ -175,6 +179,72 @@ class FourthRankIsotropicTensor3D(FourthRankIsotropicTensor):
         return m
 
 
+class LinearOperator(AbstractLinearOperator):
+    """Matrix-based linear operator (operators.pyx:195-254); keeps a shallow
+    reference to ``a`` like the reference."""
+
+    def __init__(self, a):
+        super().__init__()
+        a = np.asarray(a, dtype=np.float64)
+        if a.ndim != 2:
+            raise ValueError('a must be a 2D array')
+        self.init_sizes(a.shape[1], a.shape[0])
+        self.a = a
+
+    def _apply_host(self, x, y):
+        # y[i] = 0; y[i] += a[i, j] * x[j] in j order (operators.pyx:209-214)
+        for i in range(self.osize):
+            acc = 0.0
+            for j in range(self.isize):
+                acc += float(self.a[i, j]) * float(x[j])
+            y[i] = acc
+
+    def apply_transpose(self, x, y=None):
+        """operators.pyx:225-244"""
+        x = np.asarray(x, dtype=np.float64)
+        _check_1d(x, self.osize)
+        y = _out_1d(y, self.isize)
+        for j in range(self.isize):
+            acc = 0.0
+            for i in range(self.osize):
+                acc += float(self.a[i, j]) * float(x[i])
+            y[j] = acc
+        return y[...]
+
+    def _to_matrix(self):
+        return np.array(self.a, dtype=np.float64)
+
+
+class FourthRankCubicTensor2D(AbstractLinearOperator):
+    """Fourth-rank tensor with cubic symmetry in 2D (plane strain), rotated
+    by theta (operators.pyx:411-450), Mandel form."""
+
+    def __init__(self, t1111, t1122, t1212, theta):
+        super().__init__()
+        self.init_sizes(3, 3)
+        self.dim = 2
+        # operators.pyx:417-425, same operation order
+        c = math.cos(4 * theta)
+        s = math.sin(4 * theta)
+        aux = t1111 - t1122 - 2 * t1212
+        self.t11 = 0.25 * (3 * t1111 + t1122 + 2 * t1212 + c * aux)
+        self.t12 = 0.25 * (t1111 + 3 * t1122 - 2 * t1212 - c * aux)
+        self.t13 = 0.25 * math.sqrt(2.0) * s * aux
+        self.t23 = -self.t13
+        self.t33 = 0.50 * (t1111 - t1122 + 2 * t1212 - c * aux)
+
+    def _apply_host(self, x, y):
+        x0, x1, x2 = float(x[0]), float(x[1]), float(x[2])
+        y[0] = self.t11 * x0 + self.t12 * x1 + self.t13 * x2
+        y[1] = self.t12 * x0 + self.t11 * x1 + self.t23 * x2
+        y[2] = self.t13 * x0 + self.t23 * x1 + self.t33 * x2
+
+    def _to_matrix(self):
+        return np.array([[self.t11, self.t12, self.t13],
+                         [self.t12, self.t11, self.t23],
+                         [self.t13, self.t23, self.t33]])
+
+
 def isotropic_4(sph, dev, dim):
     """Create a FourthRankIsotropicTensor (operators.pyx:53-67)."""
     if dim == 2:
@@ -262,12 +332,18 @@ class LocalPhaseOperator:
     the phase map, for the solver and the block-diagonal operators.
 
     ``phase=None`` makes it a stiffness field: ``sph`` and ``dev`` then hold
-    one coefficient per voxel (C order over the grid), as for mu(x)."""
+    one coefficient per voxel (C order over the grid), as for mu(x).
+    ``matrices`` (nphase x s x s) replaces (sph, dev) by a full matrix per
+    entry (anisotropic phases, e.g. rotated cubic grains)."""
 
-    def __init__(self, dim, shape, phase, sph, dev, dtype=torch.float64):
+    def __init__(self, dim, shape, phase, sph, dev, dtype=torch.float64, matrices=None):
         self.dim = int(dim)
         self.shape = tuple(int(v) for v in shape)
         self.dtype = dtype
+        self.matrices = None
+        if matrices is not None:
+            self._init_matrices(phase, matrices)
+            return
         if A.is_tensor(sph):
             sph = sph.detach().cpu().numpy()
         if A.is_tensor(dev):
@@ -308,6 +384,52 @@ class LocalPhaseOperator:
             self.dim, _lib.i64_array(self.shape), self.nphase, sph.ctypes.data_as(_P),
             dev.ctypes.data_as(_P), ctypes.c_void_p(ph.data_ptr()), index_bytes,
             A.jb_dtype(dtype), ctypes.byref(self._handle)))
+
+    def _init_matrices(self, phase, matrices):
+        s = 3 if self.dim == 2 else 6
+        mats = np.ascontiguousarray(np.asarray(matrices, dtype=np.float64))
+        if mats.ndim != 3 or mats.shape[1:] != (s, s):
+            raise ValueError("matrices must have shape (nphase, {0}, {0})".format(s))
+        self.matrices = mats
+        self.sph = self.dev = None
+        self.nphase = int(mats.shape[0])
+        P = ctypes.POINTER(ctypes.c_double)
+        self._handle = ctypes.c_void_p()
+        if phase is None:
+            if self.nphase != int(np.prod(self.shape)):
+                raise ValueError("a matrix field needs one matrix per voxel")
+            self.phase = None
+            _lib.check(_lib.lib().jb_local_create_matrix(
+                self.dim, _lib.i64_array(self.shape), self.nphase, mats.ctypes.data_as(P), None,
+                0, A.jb_dtype(self.dtype), ctypes.byref(self._handle)))
+            return
+        index_bytes = 1 if self.nphase <= 256 else 4
+        ph = self._phase_map(phase, index_bytes)
+        _lib.check(_lib.lib().jb_local_create_matrix(
+            self.dim, _lib.i64_array(self.shape), self.nphase, mats.ctypes.data_as(P),
+            ctypes.c_void_p(ph.data_ptr()), index_bytes, A.jb_dtype(self.dtype),
+            ctypes.byref(self._handle)))
+
+    def _phase_map(self, phase, index_bytes):
+        if A.is_tensor(phase):
+            ph = phase.to(A.device())
+        else:
+            ph = torch.from_numpy(np.ascontiguousarray(np.asarray(phase))).to(A.device())
+        if tuple(ph.shape) != self.shape:
+            raise ValueError("phase map shape {} differs from grid {}".format(
+                tuple(ph.shape), self.shape))
+        if ph.numel() and (int(ph.min()) < 0 or int(ph.max()) >= self.nphase):
+            raise ValueError("phase indices must lie in [0, {})".format(self.nphase))
+        ph = ph.to(torch.uint8 if index_bytes == 1 else torch.int32).contiguous()
+        self.phase = ph
+        return ph
+
+    def with_dtype(self, dtype):
+        """The same operator in another precision."""
+        if self.matrices is not None:
+            return LocalPhaseOperator(self.dim, self.shape, self.phase, None, None, dtype,
+                                      matrices=self.matrices)
+        return LocalPhaseOperator(self.dim, self.shape, self.phase, self.sph, self.dev, dtype)
 
     @property
     def handle(self):
@@ -392,9 +514,14 @@ class _BlockDiagonalOperator:
                 if not hasattr(op, "to_memoryview"):
                     raise TypeError("local operators must be linear (define to_memoryview)")
                 mats.append(np.asarray(op.to_memoryview(), dtype=np.float64))
-            table = torch.from_numpy(np.stack(mats)).to(A.device(), self._dtype)
-            idx = torch.from_numpy(phase.ravel()).to(A.device())
-            self._matrices = table[idx].contiguous()
+            if ilast == olast and ilast == (3 if self._ndim == 2 else 6):
+                # square Mandel blocks: a phase map + matrix table (solver-ready)
+                self._local = LocalPhaseOperator(self._ndim, self._shape, phase, None, None,
+                                                 self._dtype, matrices=np.stack(mats))
+            else:
+                table = torch.from_numpy(np.stack(mats)).to(A.device(), self._dtype)
+                idx = torch.from_numpy(phase.ravel()).to(A.device())
+                self._matrices = table[idx].contiguous()
 
     @classmethod
     def from_phases(cls, phase, ops, dtype=None):
@@ -409,15 +536,22 @@ class _BlockDiagonalOperator:
         op0 = ops[0]
         obj.init_shapes(*phase_shape, op0.isize, op0.osize)
         obj._dtype = A.torch_dtype(dtype)
-        for op in ops:
-            if not (isinstance(op, FourthRankIsotropicTensor) and op.dim == cls._ndim):
-                raise TypeError("from_phases expects FourthRankIsotropicTensor{0}D "
-                                "operators".format(cls._ndim))
         obj.loc = None
         obj._matrices = None
-        obj._local = LocalPhaseOperator(cls._ndim, phase_shape, phase,
-                                        [op.sph for op in ops], [op.dev for op in ops],
-                                        obj._dtype)
+        if all(isinstance(op, FourthRankIsotropicTensor) and op.dim == cls._ndim
+               for op in ops):
+            obj._local = LocalPhaseOperator(cls._ndim, phase_shape, phase,
+                                            [op.sph for op in ops], [op.dev for op in ops],
+                                            obj._dtype)
+            return obj
+        s = 3 if cls._ndim == 2 else 6
+        mats = []
+        for op in ops:
+            if not hasattr(op, "to_memoryview") or op.isize != s or op.osize != s:
+                raise TypeError("from_phases expects {0} x {0} linear local operators".format(s))
+            mats.append(np.asarray(op.to_memoryview(), dtype=np.float64))
+        obj._local = LocalPhaseOperator(cls._ndim, phase_shape, phase, None, None, obj._dtype,
+                                        matrices=np.stack(mats))
         return obj
 
     @property

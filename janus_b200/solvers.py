@@ -195,8 +195,7 @@ class MixedScheme:
         self.inner = int(inner)
         self.green32 = type(green_op)(green_op.green, green_op.ishape[:-1], green_op.h,
                                       dtype=torch.float32)
-        self.local32 = LocalPhaseOperator(local.dim, local.shape, local.phase, local.sph,
-                                          local.dev, dtype=torch.float32)
+        self.local32 = local.with_dtype(torch.float32)
         if method not in self.METHODS:
             raise ValueError("method must be 'basic' or 'bicgstab'")
         self.method = method

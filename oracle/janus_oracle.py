@@ -347,6 +347,20 @@ def phase_apply(x, phase, sph_table, dev_table, dim) -> np.ndarray:
     return isotropic_apply(x, sph, dev, dim)
 
 
+def cubic2d_matrix(t1111, t1122, t1212, theta) -> np.ndarray:
+    """Mandel matrix of FourthRankCubicTensor2D (operators.pyx:413-450), same
+    operation order."""
+    c = math.cos(4 * theta)
+    s = math.sin(4 * theta)
+    aux = t1111 - t1122 - 2 * t1212
+    t11 = 0.25 * (3 * t1111 + t1122 + 2 * t1212 + c * aux)
+    t12 = 0.25 * (t1111 + 3 * t1122 - 2 * t1212 - c * aux)
+    t13 = 0.25 * math.sqrt(2.0) * s * aux
+    t23 = -t13
+    t33 = 0.50 * (t1111 - t1122 + 2 * t1212 - c * aux)
+    return np.array([[t11, t12, t13], [t12, t11, t23], [t13, t23, t33]])
+
+
 def block_linear_apply(a, x, transpose=False) -> np.ndarray:
     """BlockDiagonalLinearOperator{2,3}D.c_apply / c_apply_transpose
     (operators.pyx:739-774, 823-861): y[v,i] = sum_j a[v,i,j] x[v,j] summed in
@@ -366,7 +380,7 @@ def block_linear_apply(a, x, transpose=False) -> np.ndarray:
 # --------------------------------------------------------------------------
 
 def basic_scheme(phase, sph_table, dev_table, g0, nu0, avg_eps, num_iter,
-                 h=1.0, variant="truncated", tol=None, callback=None):
+                 h=1.0, variant="truncated", tol=None, callback=None, mats=None):
     """The tutorial loop square_basic.py:83-97 with a phase-map local operator.
 
     eps0 = E; eps_{k+1} = E - Gamma0[(C - C0):eps_k];
@@ -374,19 +388,30 @@ def basic_scheme(phase, sph_table, dev_table, g0, nu0, avg_eps, num_iter,
     Stops after ``num_iter`` iterations, or earlier once res_k <= tol.
     Returns (eps, residuals, mean_tau) where mean_tau is the mean of
     (C - C0):eps over the grid for the final eps (square_basic.py:95-96).
+    With ``mats`` (nphase x s x s), phase p's local operator is the matrix
+    mats[p] (BlockDiagonalOperator over LinearOperator / cubic tensors)
+    instead of isotropic_4(sph[p], dev[p]).
     """
     phase = np.asarray(phase)
     n = phase.shape
     dim = len(n)
     avg_eps = np.asarray(avg_eps, dtype=np.float64)
     G = spectral_green_field(n, h, g0, nu0, variant)
+    if mats is not None:
+        mats = np.asarray(mats, dtype=np.float64)
+
+        def local(x):
+            return block_linear_apply(mats[phase], x)
+    else:
+        def local(x):
+            return phase_apply(x, phase, sph_table, dev_table, dim)
     eps = np.empty(n + (avg_eps.shape[0],))
     eps[...] = avg_eps
     num_cells = int(np.prod(n))
     normalization = 1 / np.sqrt(num_cells) / np.linalg.norm(avg_eps)
     res = []
     for it in range(num_iter):
-        tau = phase_apply(eps, phase, sph_table, dev_table, dim)
+        tau = local(eps)
         y = green_apply(tau, g0, nu0, h, variant, G=G)
         new_eps = avg_eps - y
         res.append(normalization * np.linalg.norm(new_eps - eps))
@@ -395,7 +420,7 @@ def basic_scheme(phase, sph_table, dev_table, g0, nu0, avg_eps, num_iter,
             callback(it, eps)
         if tol is not None and res[-1] <= tol:
             break
-    tau = phase_apply(eps, phase, sph_table, dev_table, dim)
+    tau = local(eps)
     mean_tau = np.mean(tau, axis=tuple(range(dim)))
     return eps, np.asarray(res), mean_tau
 

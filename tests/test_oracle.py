@@ -190,3 +190,36 @@ def test_oracle_adjoint_gradient_matches_differences(cot):
             vals.append(G @ O.field_mean_stress(m, nu, g0, nu, E, its, tol))
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - grad.flat[v]) <= 1e-6 * abs(grad).max(), (v, fd, grad.flat[v])
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.3, 1.1, -2.0])
+def test_oracle_cubic_tensor_matches_reference_build(theta):
+    ref = reference_checker()
+    if ref is None:
+        pytest.skip("reference checker (oracle/_ref) not built")
+    import janus.operators as rops
+    t = rops.FourthRankCubicTensor2D(3.0, 1.2, 0.7, theta)
+    np.testing.assert_array_equal(np.asarray(t.to_memoryview()),
+                                  O.cubic2d_matrix(3.0, 1.2, 0.7, theta))
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.7])
+def test_host_linear_and_cubic_operators_match_reference_build(theta):
+    """janus_b200.operators.LinearOperator / FourthRankCubicTensor2D (host
+    apply, to_memoryview) against the reference's compiled classes, bitwise."""
+    ref = reference_checker()
+    if ref is None:
+        pytest.skip("reference checker (oracle/_ref) not built")
+    import janus.operators as rops
+    from janus_b200 import operators as mops
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(3)
+    a = rng.standard_normal((3, 3))
+    r_cub, m_cub = rops.FourthRankCubicTensor2D(3.0, 1.2, 0.7, theta), \
+        mops.FourthRankCubicTensor2D(3.0, 1.2, 0.7, theta)
+    np.testing.assert_array_equal(np.asarray(r_cub.apply(x)), m_cub.apply(x))
+    np.testing.assert_array_equal(np.asarray(r_cub.to_memoryview()), m_cub.to_memoryview())
+    r_lin, m_lin = rops.LinearOperator(a), mops.LinearOperator(a)
+    np.testing.assert_array_equal(np.asarray(r_lin.apply(x)), m_lin.apply(x))
+    np.testing.assert_array_equal(np.asarray(r_lin.apply_transpose(x)), m_lin.apply_transpose(x))
+    np.testing.assert_array_equal(np.asarray(r_lin.to_memoryview()), m_lin.to_memoryview())
