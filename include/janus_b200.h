@@ -136,8 +136,11 @@ int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
  * compile-time tiles allowed, Green width, Green input tiles, Green
  * compile-time tiles allowed}; widths in complex columns (the Green one a
  * multiple of s), input tiles 2 or 3, 0 = built-in rule.  A width whose
- * tiles do not fit the shared-memory budget is narrowed.  Set by the
- * autotuner (janus_b200.autotune) from timed candidates. */
+ * tiles do not fit the shared-memory budget is narrowed.  An optional 7th
+ * value selects the Green contraction: 0 built-in rule (the M/N table for
+ * the filtered operator, on the fly for the truncated and finite-difference
+ * ones), 1 the M/N table, 2 on the fly.  Set by the autotuner
+ * (janus_b200.autotune) from timed candidates; count is 6 or 7. */
 int jb_green_set_tuning(jb_green *green, const int *v, int count);
 int jb_green_get_tuning(jb_green *green, int *v, int count);
 /* set_frequency + to_memoryview at index b (green.pyx:146-171, 312-342 and

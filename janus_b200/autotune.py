@@ -5,8 +5,9 @@ No counterpart in the reference, which leaves planning to FFTW
 FFT radices follow from the axis length (compile-time radix-16/8 tiles for
 n = 64, 128, 256; runtime mixed-radix plans otherwise); what is tuned is how
 the column passes tile the spectrum: the width of a tile in complex columns,
-how many input tiles rotate through shared memory, and whether the
-compile-time tiles are used.  Each candidate is timed on the solver step it
+how many input tiles rotate through shared memory, whether the compile-time
+tiles are used, and whether the Green contraction reads the per-coefficient
+M/N table or evaluates the operator on the fly.  Each candidate is timed on the solver step it
 will serve (CUDA events around every pass, several steps after a warm-up),
 the plain passes (3D axis 1) and the Green pass independently, and the
 fastest of each is set on the operator.  Results are cached per GPU model,
@@ -30,14 +31,19 @@ _GREEN_PASS = "cols_green_axis0"
 
 
 def get_tuning(green_op):
-    v = (ctypes.c_int * 6)()
-    _lib.check(_lib.lib().jb_green_get_tuning(green_op.handle, v, 6))
+    """[plain width, plain input tiles, plain compile-time, Green width,
+    Green input tiles, Green compile-time, contraction mode]"""
+    v = (ctypes.c_int * 7)()
+    _lib.check(_lib.lib().jb_green_get_tuning(green_op.handle, v, 7))
     return list(v)
 
 
 def set_tuning(green_op, values):
-    v = (ctypes.c_int * 6)(*[int(x) for x in values])
-    _lib.check(_lib.lib().jb_green_set_tuning(green_op.handle, v, 6))
+    """6 values (schedules) or 7 (with the contraction mode: 0 rule, 1
+    M/N table, 2 on the fly)."""
+    values = [int(x) for x in values]
+    v = (ctypes.c_int * len(values))(*values)
+    _lib.check(_lib.lib().jb_green_set_tuning(green_op.handle, v, len(values)))
 
 
 def candidates(dim, dtype):
@@ -98,8 +104,8 @@ def tune(green_op, local_op, nload=1, steps=5, warmup=2, use_cache=True):
         (nload,) + (1,) * dim + (s,))
     res = torch.zeros(nload, dtype=torch.float64, device=eps.device)
     plain_c, green_c = candidates(dim, green_op.dtype)
-    base = get_tuning(green_op)
-    best_plain, best_green = (base[0:3], float("inf")), (base[3:6], float("inf"))
+    base = get_tuning(green_op)[:6]
+    best_plain, best_green = (base[0:3], float("inf")), (base[3:6] + [0], float("inf"))
     # plain passes (3D): vary the plain schedule, Green schedule fixed
     for c in plain_c:
         set_tuning(green_op, list(c) + base[3:6])
@@ -107,12 +113,13 @@ def tune(green_op, local_op, nload=1, steps=5, warmup=2, use_cache=True):
         ms = sum(t.get(p, 0.0) for p in _PLAIN_PASSES)
         if ms < best_plain[1]:
             best_plain = (list(c), ms)
-    for c in green_c:
-        set_tuning(green_op, best_plain[0] + list(c))
-        t = _time_passes(solver, eps, res, steps, warmup)
-        ms = t.get(_GREEN_PASS, float("inf"))
-        if ms < best_green[1]:
-            best_green = (list(c), ms)
+    for mode in (1, 2):   # M/N table, on the fly
+        for c in green_c:
+            set_tuning(green_op, best_plain[0] + list(c) + [mode])
+            t = _time_passes(solver, eps, res, steps, warmup)
+            ms = t.get(_GREEN_PASS, float("inf"))
+            if ms < best_green[1]:
+                best_green = (list(c) + [mode], ms)
     chosen = best_plain[0] + best_green[0]
     set_tuning(green_op, chosen)
     out = {"tuning": chosen, "plain_ms": best_plain[1] if plain_c else None,

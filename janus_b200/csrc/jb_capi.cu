@@ -256,6 +256,7 @@ struct jb_green_s {
   DeviceBuf bidx;
   DeviceBuf mnbuf;        // per-coefficient M/N table, built on first use
   jb::ColsTuning tune_plain, tune_green;  // column-pass schedules (autotuner)
+  int tune_table = 0;  // Green contraction: 0 built-in rule, 1 M/N table, 2 on the fly
   bool use_table = true;  // false: evaluate the operator on the fly
 };
 
@@ -324,6 +325,14 @@ int upload_table(jb_green* g, int dtype, const std::vector<double>& v, void** ou
 
 // spectral passes shared by jb_green_apply and the solver
 // x: real fields (or eps with local), spec: complex scratch, y: output
+// whether the Green pass contracts through the M/N table (else on the fly):
+// the tuned choice, or the built-in rule (the table for the filtered
+// operator's 2^d aliases per coefficient, on the fly for one alias)
+bool green_uses_table(const jb_green* g) {
+  return g->use_table &&
+         (g->tune_table == 1 || (g->tune_table == 0 && g->variant == JB_FILTERED));
+}
+
 // the operator's M/N tensors at every half-spectrum coefficient, built once
 // on first use (or ahead of a graph capture)
 int green_prepare(jb_green* g, cudaStream_t st) {
@@ -379,9 +388,19 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
     rec->mark(st);
   }
   const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
-  JB_TRY(green_prepare(g, st));
+  // the contraction reads the M/N table (built once) or evaluates the
+  // operator on the fly; built-in rule: the table for the filtered operator
+  // (2^d aliases per coefficient), on the fly for the single-alias ones
+  const bool table = green_uses_table(g);
+  jb::GreenDeviceTables gt = g->gt;
+  if (table) {
+    JB_TRY(green_prepare(g, st));
+    gt.mn = g->gt.mn;
+  } else {
+    gt.mn = nullptr;
+  }
   JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
-                                       &g->gt, n1, m, st, &g->tune_green),
+                                       &gt, n1, m, st, &g->tune_green),
                        "cols_green_axis0"));
   rec->mark(st);
   if (dim == 3) {
@@ -676,7 +695,9 @@ int jb_green_destroy(jb_green* G) {
 
 int jb_green_set_tuning(jb_green* G, const int* v, int count) {
   if (!G || !v) return fail(JB_EINVAL, "NULL argument");
-  if (count != 6) return fail(JB_EINVAL, "tuning takes 6 values");
+  if (count != 6 && count != 7) return fail(JB_EINVAL, "tuning takes 6 or 7 values");
+  if (count == 7 && (v[6] < 0 || v[6] > 2))
+    return fail(JB_EINVAL, "contraction mode must be 0 (rule), 1 (table) or 2 (on the fly)");
   const int C = G->dim == 2 ? 3 : 6;
   if (v[0] < 0 || v[0] > 128 || v[3] < 0 || v[3] > 128 || (v[3] % C) != 0)
     return fail(JB_EINVAL, "tile widths must be in [0, 128], the Green one a multiple of s");
@@ -688,12 +709,14 @@ int jb_green_set_tuning(jb_green* G, const int* v, int count) {
   G->tune_green.w = v[3];
   G->tune_green.nbuf = v[4];
   G->tune_green.ct = v[5] != 0;
+  if (count == 7) G->tune_table = v[6];
   return JB_OK;
 }
 
 int jb_green_get_tuning(jb_green* G, int* v, int count) {
   if (!G || !v) return fail(JB_EINVAL, "NULL argument");
-  if (count != 6) return fail(JB_EINVAL, "tuning takes 6 values");
+  if (count != 6 && count != 7) return fail(JB_EINVAL, "tuning takes 6 or 7 values");
+  if (count == 7) v[6] = G->tune_table;
   v[0] = G->tune_plain.w;
   v[1] = G->tune_plain.nbuf;
   v[2] = G->tune_plain.ct;
@@ -1745,7 +1768,8 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
     eoff += (size_t)M->L * C;
   }
   for (size_t i = 0; i < P; ++i) {
-    JB_TRY(green_prepare(B->prob[i]->g32, st));  // nothing lazily built inside a capture
+    if (green_uses_table(B->prob[i]->g32))  // nothing lazily built inside a capture
+      JB_TRY(green_prepare(B->prob[i]->g32, st));
     if (B->prob[i]->method == JB_INNER_BICGSTAB) JB_TRY(mixed_krylov_buffers(B->prob[i]));
     JB_TRY(mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st));
   }

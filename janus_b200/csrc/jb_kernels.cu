@@ -1529,8 +1529,9 @@ cudaError_t cols_ct_dispatch(int mode, int dim, const CUtensorMap& tin, const CU
                              cudaStream_t st) {
   if (mode == 0) return cols_ct_launch<T, 0, 2, N, 8>(tin, tout, a, nbox, smem, tiles, st);
   if (mode == 1) return cols_ct_launch<T, 1, 2, N, 8>(tin, tout, a, nbox, smem, tiles, st);
-  if constexpr (N == 256) {
-    // six-column Green tiles: the width FP64 tiles of 256 rows fit
+  if constexpr (N == 128 || N == 256) {
+    // six-column Green tiles (one 3D coefficient, two 2D ones): the width
+    // FP64 tiles of 256 rows fit; at 128 rows an autotuner candidate
     if (a.W == 6) {
       if (dim == 2) return cols_ct_launch<T, 2, 2, N, 6>(tin, tout, a, nbox, smem, tiles, st);
       return cols_ct_launch<T, 2, 3, N, 6>(tin, tout, a, nbox, smem, tiles, st);
@@ -1593,7 +1594,7 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
         b.nbuf = nbuf;
         const int thr = tile_threads(Wp);
         const int64_t tiles = (inner + Wp - 1) / Wp * outer;
-        const bool ct_w = (mode == 2 ? (Wp == 12 || (Wp == 6 && n == 256)) : Wp == 8) &&
+        const bool ct_w = (mode == 2 ? (Wp == 12 || (Wp == 6 && n >= 128)) : Wp == 8) &&
                           (mode != 2 || C == 3 || C == 6);
         if (ct_w && (!tune || tune->ct)) {
           if (n == 64) return cols_ct_dispatch<T, 64>(mode, dim, tin, tout, b, nbox, sp, tiles, st);

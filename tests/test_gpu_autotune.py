@@ -38,10 +38,11 @@ def test_every_candidate_computes_the_same_operator(dim, n, dtype):
         autotune.set_tuning(g, list(c) + base[3:6])
         y = g.apply(x).double().cpu().numpy()
         assert np.abs(y - ref).max() <= tol * np.abs(ref).max(), c
-    for c in green:
-        autotune.set_tuning(g, base[0:3] + list(c))
-        y = g.apply(x).double().cpu().numpy()
-        assert np.abs(y - exact).max() <= tol * np.abs(exact).max(), c
+    for mode in (1, 2):   # M/N table, on the fly
+        for c in green:
+            autotune.set_tuning(g, base[0:3] + list(c) + [mode])
+            y = g.apply(x).double().cpu().numpy()
+            assert np.abs(y - exact).max() <= tol * np.abs(exact).max(), (c, mode)
 
 
 @pytest.mark.gpu
@@ -52,7 +53,11 @@ def test_tuning_validation():
     with pytest.raises(ValueError):
         autotune.set_tuning(g, [8, 4, 1, 12, 2, 1])  # 4 input tiles
     autotune.set_tuning(g, [16, 3, 0, 18, 2, 1])
-    assert autotune.get_tuning(g) == [16, 3, 0, 18, 2, 1]
+    assert autotune.get_tuning(g) == [16, 3, 0, 18, 2, 1, 0]
+    autotune.set_tuning(g, [16, 3, 0, 18, 2, 1, 2])
+    assert autotune.get_tuning(g) == [16, 3, 0, 18, 2, 1, 2]
+    with pytest.raises(ValueError):
+        autotune.set_tuning(g, [8, 2, 1, 12, 2, 1, 3])
 
 
 @pytest.mark.gpu
@@ -70,7 +75,7 @@ def test_tune_sets_and_caches(dim, tmp_path, monkeypatch):
     assert not r1["cached"]
     assert autotune.get_tuning(g) == r1["tuning"]
     plain, green = autotune.candidates(dim, torch.float64)
-    assert tuple(r1["tuning"][3:6]) in green
+    assert tuple(r1["tuning"][3:6]) in green and r1["tuning"][6] in (1, 2)
     if dim == 3:
         assert tuple(r1["tuning"][0:3]) in plain
     g2 = _green(dim, n, "filtered", torch.float64)
