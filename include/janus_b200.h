@@ -241,12 +241,16 @@ int jb_mixed_create(jb_green *g64, jb_local *l64, jb_green *g32, jb_local *l32,
 int jb_mixed_destroy(jb_mixed *solver);
 /* Inner solver of the correction equation A d = r, A d = d + Gamma0[(C -
  * C0):d] (the basic scheme's operator, FP32): JB_INNER_BASIC runs `inner - 1`
- * basic iterations (the default); JB_INNER_BICGSTAB runs `inner` BiCGSTAB
- * iterations (two applications of A each) from d = 0, batched over the load
- * cases with device-side scalars.  The outer FP64 residual and stopping test
- * are the same for both; fp32_iters_out counts applications of A. */
+ * basic iterations (the default); JB_INNER_BICGSTAB runs up to `inner`
+ * BiCGSTAB iterations (two applications of A each) from d = 0, batched over
+ * the load cases with device-side scalars: after the first correction,
+ * jb_mixed_run sizes each one by the residual reduction per iteration seen
+ * over the previous one, extrapolated to half the tolerance (jb_batch_run
+ * always runs `inner`).  The outer FP64 residual and stopping test are the
+ * same for both; fp32_iters_out counts applications of A. */
 #define JB_INNER_BASIC 0
 #define JB_INNER_BICGSTAB 1
+#define JB_INNER_BICGSTAB_FIXED 2 /* always `inner` iterations per correction */
 int jb_mixed_set_method(jb_mixed *solver, int method);
 /* eps: device double[nload][grid][s]; E host double[nload][s]; residuals:
  * host double[max_outer][nload] (FP64 residual at each outer step, may be

@@ -1405,8 +1405,10 @@ extern "C" int jb_mixed_create(jb_green* g64, jb_local* l64, jb_green* g32, jb_l
 
 extern "C" int jb_mixed_set_method(jb_mixed* M, int method) {
   if (!M) return fail(JB_EINVAL, "NULL argument");
-  if (method != JB_INNER_BASIC && method != JB_INNER_BICGSTAB)
-    return fail(JB_EINVAL, "method must be JB_INNER_BASIC or JB_INNER_BICGSTAB");
+  if (method != JB_INNER_BASIC && method != JB_INNER_BICGSTAB &&
+      method != JB_INNER_BICGSTAB_FIXED)
+    return fail(JB_EINVAL,
+                "method must be JB_INNER_BASIC, JB_INNER_BICGSTAB or JB_INNER_BICGSTAB_FIXED");
   M->method = method;
   return JB_OK;
 }
@@ -1585,22 +1587,40 @@ extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, i
   JB_TRY(mixed_set_load(M, E, eps, init, st));
   std::vector<double> r(L);
   int outer = 0, fp32 = 0;
+  double rprev = 0.0;  // largest residual of the previous outer step
+  int kprev = 0;       // Krylov iterations of the previous correction
   for (; outer < max_outer; ++outer) {
     JB_TRY(mixed_residual(M, eps, static_cast<double*>(M->res.p), st));
     JB_CUDA(cudaMemcpyAsync(r.data(), M->res.p, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
     JB_CUDA(cudaStreamSynchronize(st));
     bool done = true;
+    double rmax = 0.0;
     for (int l = 0; l < L; ++l) {
       if (residuals) residuals[(size_t)outer * L + l] = r[l];
       if (!(r[l] <= tol)) done = false;
+      rmax = std::max(rmax, r[l]);
     }
     if (done) {
       ++outer;
       break;
     }
-    if (M->method == JB_INNER_BICGSTAB) {
-      JB_TRY(mixed_correct_bicgstab(M, eps, inner, st));
-      fp32 += 2 * inner;
+    if (M->method == JB_INNER_BICGSTAB || M->method == JB_INNER_BICGSTAB_FIXED) {
+      // iterations this correction needs: the reduction per iteration seen
+      // over the previous correction, extrapolated to half the tolerance
+      // (at most `inner`; the full count when no rate is known yet)
+      int k = inner;
+      if (M->method == JB_INNER_BICGSTAB && kprev > 0 && rprev > 0.0 && rmax > 0.0 &&
+          rmax < rprev) {
+        const double rate = std::pow(rmax / rprev, 1.0 / kprev);
+        if (rate > 0.0 && rate < 1.0) {
+          const double need = std::log(0.5 * tol / rmax) / std::log(rate);
+          if (need > 0.0 && need + 2.0 < (double)inner) k = std::max(2, (int)std::ceil(need) + 2);
+        }
+      }
+      JB_TRY(mixed_correct_bicgstab(M, eps, k, st));
+      fp32 += 2 * k;
+      rprev = rmax;
+      kprev = k;
     } else {
       JB_TRY(mixed_correct(M, eps, inner, st));
       fp32 += inner - 1;
@@ -1707,7 +1727,7 @@ int batch_capture(jb_batch* B, const std::vector<char>& active, void* const* eps
   for (size_t i = 0; i < B->prob.size() && r == JB_OK && e == cudaSuccess; ++i) {
     if (!active[i]) continue;
     cudaStream_t st = B->streams[B->branch[i] + 1];
-    r = B->prob[i]->method == JB_INNER_BICGSTAB
+    r = B->prob[i]->method != JB_INNER_BASIC
             ? mixed_correct_bicgstab(B->prob[i], eps[i], inner, st)
             : mixed_correct(B->prob[i], eps[i], inner, st);
     if (r == JB_OK) r = mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st);
@@ -1770,7 +1790,7 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
   for (size_t i = 0; i < P; ++i) {
     if (green_uses_table(B->prob[i]->g32))  // nothing lazily built inside a capture
       JB_TRY(green_prepare(B->prob[i]->g32, st));
-    if (B->prob[i]->method == JB_INNER_BICGSTAB) JB_TRY(mixed_krylov_buffers(B->prob[i]));
+    if (B->prob[i]->method != JB_INNER_BASIC) JB_TRY(mixed_krylov_buffers(B->prob[i]));
     JB_TRY(mixed_residual(B->prob[i], eps[i], res + B->res_off[i], st));
   }
   std::vector<double> rh(B->nres);
@@ -1826,7 +1846,7 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
     if (outer_out) outer_out[i] = outer[i];
     if (fp32_iters_out)
       fp32_iters_out[i] =
-          (outer[i] - 1) * (M->method == JB_INNER_BICGSTAB ? 2 * inner : inner - 1);
+          (outer[i] - 1) * (M->method != JB_INNER_BASIC ? 2 * inner : inner - 1);
     if (mean_tau) JB_TRY(mixed_mean(M, eps[i], mean_tau + eoff, st));
     eoff += (size_t)M->L * C;
   }

@@ -24,6 +24,15 @@ namespace {
 
 constexpr int kKrThreads = 256;
 
+// four consecutive elements per access (16 bytes FP32, 2 x 16 bytes FP64)
+template <typename T> struct V4;
+template <> struct V4<float> {
+  using type = float4;
+};
+template <> struct V4<double> {
+  using type = double4;
+};
+
 __device__ __forceinline__ double kr_block_sum(double v, double* red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -39,6 +48,15 @@ __device__ __forceinline__ double kr_block_sum(double v, double* red) {
 
 __device__ __forceinline__ bool kr_finite(double v) { return isfinite(v); }
 
+// vector accesses apply when every field of the load case starts on a
+// 16-byte (FP32) / 32-byte (FP64) boundary; the tail runs scalar
+template <typename T>
+__device__ __forceinline__ bool kr_vec4(int64_t nel, const T* a, const T* b, const T* c) {
+  const uintptr_t m = (uintptr_t)(4 * sizeof(T) - 1);
+  return nel >= 4 && ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) |
+                       reinterpret_cast<uintptr_t>(c)) & m) == 0;
+}
+
 // partials[(l * 2 + q) * nb + b] of a.b (q = 0) and c.d (q = 1, if c)
 template <typename T>
 __global__ void __launch_bounds__(kKrThreads)
@@ -48,8 +66,27 @@ __global__ void __launch_bounds__(kKrThreads)
   const int l = blockIdx.y, nb = gridDim.x;
   const int64_t off = (int64_t)l * nel;
   double s0 = 0.0, s1 = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
-       i += (int64_t)nb * blockDim.x) {
+  const int64_t stride = (int64_t)nb * blockDim.x;
+  int64_t i0 = 0;
+  if (kr_vec4(nel, a + off, b + off, c ? c + off : a + off) &&
+      kr_vec4(nel, d ? d + off : a + off, a + off, a + off)) {
+    using V = typename V4<T>::type;
+    const V* a4 = reinterpret_cast<const V*>(a + off);
+    const V* b4 = reinterpret_cast<const V*>(b + off);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel / 4; i += stride) {
+      const V x = a4[i], y = b4[i];
+      s0 += (double)x.x * (double)y.x + (double)x.y * (double)y.y + (double)x.z * (double)y.z +
+            (double)x.w * (double)y.w;
+      if (c) {
+        const V u = reinterpret_cast<const V*>(c + off)[i];
+        const V w = reinterpret_cast<const V*>(d + off)[i];
+        s1 += (double)u.x * (double)w.x + (double)u.y * (double)w.y + (double)u.z * (double)w.z +
+              (double)u.w * (double)w.w;
+      }
+    }
+    i0 = nel / 4 * 4;
+  }
+  for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel; i += stride) {
     s0 += (double)a[off + i] * (double)b[off + i];
     if (c) s1 += (double)c[off + i] * (double)d[off + i];
   }
@@ -117,8 +154,25 @@ __global__ void kr_update_p_kernel(int64_t nel, const T* __restrict__ r, const T
   const double beta = (k.rho1 / k.rho) * (k.alpha / k.omega);
   const T b = (T)beta, om = (T)k.omega;
   const int64_t off = (int64_t)l * nel;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
-       i += (int64_t)gridDim.x * blockDim.x)
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i0 = 0;
+  if (kr_vec4(nel, r + off, v + off, p + off)) {
+    using V = typename V4<T>::type;
+    const V* r4 = reinterpret_cast<const V*>(r + off);
+    const V* v4 = reinterpret_cast<const V*>(v + off);
+    V* p4 = reinterpret_cast<V*>(p + off);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel / 4; i += stride) {
+      const V rr = r4[i], vv = v4[i];
+      V pp = p4[i];
+      pp.x = rr.x + b * (pp.x - om * vv.x);
+      pp.y = rr.y + b * (pp.y - om * vv.y);
+      pp.z = rr.z + b * (pp.z - om * vv.z);
+      pp.w = rr.w + b * (pp.w - om * vv.w);
+      p4[i] = pp;
+    }
+    i0 = nel / 4 * 4;
+  }
+  for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel; i += stride)
     p[off + i] = r[off + i] + b * (p[off + i] - om * v[off + i]);
 }
 
@@ -131,8 +185,25 @@ __global__ void kr_update_s_kernel(int64_t nel, const T* __restrict__ r, const T
   if (k.active != 1) return;
   const T a = (T)k.alpha;
   const int64_t off = (int64_t)l * nel;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
-       i += (int64_t)gridDim.x * blockDim.x)
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i0 = 0;
+  if (kr_vec4(nel, r + off, v + off, s + off)) {
+    using V = typename V4<T>::type;
+    const V* r4 = reinterpret_cast<const V*>(r + off);
+    const V* v4 = reinterpret_cast<const V*>(v + off);
+    V* s4 = reinterpret_cast<V*>(s + off);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel / 4; i += stride) {
+      const V rr = r4[i], vv = v4[i];
+      V o;
+      o.x = rr.x - a * vv.x;
+      o.y = rr.y - a * vv.y;
+      o.z = rr.z - a * vv.z;
+      o.w = rr.w - a * vv.w;
+      s4[i] = o;
+    }
+    i0 = nel / 4 * 4;
+  }
+  for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel; i += stride)
     s[off + i] = r[off + i] - a * v[off + i];
 }
 
@@ -149,8 +220,37 @@ __global__ void __launch_bounds__(kKrThreads)
   double acc = 0.0;
   if (k.active != 0) {
     const T a = (T)k.alpha, om = (T)k.omega;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel;
-         i += (int64_t)nb * blockDim.x) {
+    const int64_t stride = (int64_t)nb * blockDim.x;
+    int64_t i0 = 0;
+    if (kr_vec4(nel, x + off, p + off, s + off) && kr_vec4(nel, t + off, r + off, rh + off)) {
+      using V = typename V4<T>::type;
+      V* x4 = reinterpret_cast<V*>(x + off);
+      V* r4 = reinterpret_cast<V*>(r + off);
+      const V* p4 = reinterpret_cast<const V*>(p + off);
+      const V* s4 = reinterpret_cast<const V*>(s + off);
+      const V* t4 = reinterpret_cast<const V*>(t + off);
+      const V* h4 = reinterpret_cast<const V*>(rh + off);
+      for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel / 4;
+           i += stride) {
+        V xx = x4[i];
+        const V pp = p4[i], ss = s4[i], tt = t4[i], hh = h4[i];
+        xx.x += a * pp.x + om * ss.x;
+        xx.y += a * pp.y + om * ss.y;
+        xx.z += a * pp.z + om * ss.z;
+        xx.w += a * pp.w + om * ss.w;
+        x4[i] = xx;
+        V rn;
+        rn.x = ss.x - om * tt.x;
+        rn.y = ss.y - om * tt.y;
+        rn.z = ss.z - om * tt.z;
+        rn.w = ss.w - om * tt.w;
+        r4[i] = rn;
+        acc += (double)hh.x * (double)rn.x + (double)hh.y * (double)rn.y +
+               (double)hh.z * (double)rn.z + (double)hh.w * (double)rn.w;
+      }
+      i0 = nel / 4 * 4;
+    }
+    for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel; i += stride) {
       x[off + i] += a * p[off + i] + om * s[off + i];
       const T rn = s[off + i] - om * t[off + i];
       r[off + i] = rn;

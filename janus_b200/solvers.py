@@ -172,13 +172,15 @@ class MixedScheme:
     BasicScheme), solves the correction equation d + Gamma0[(C - C0):d] = r
     approximately in FP32 and adds d to the FP64 strain field.  The inner
     solver is ``method="basic"`` (``inner - 1`` basic iterations from d = r)
-    or ``method="bicgstab"`` (``inner`` BiCGSTAB iterations from d = 0, the
-    Krylov route of the reference's examples/square_inclusion_scipy.py,
-    which hands the same operator to scipy's gmres).  The FP32 operators are
+    or ``method="bicgstab"`` (up to ``inner`` BiCGSTAB iterations from
+    d = 0, sized after the first correction by the residual reduction rate
+    seen over the previous one; ``"bicgstab_fixed"`` always runs ``inner``):
+    the Krylov route of the reference's examples/square_inclusion_scipy.py,
+    which hands the same operator to scipy's gmres.  The FP32 operators are
     built from the given FP64 ones (same material, grid, discretisation and
     phase map)."""
 
-    METHODS = {"basic": 0, "bicgstab": 1}
+    METHODS = {"basic": 0, "bicgstab": 1, "bicgstab_fixed": 2}
 
     def __init__(self, green_op, local_op, nload=1, inner=20, method="basic"):
         if isinstance(local_op, _BlockDiagonalOperator):
@@ -197,7 +199,7 @@ class MixedScheme:
                                       dtype=torch.float32)
         self.local32 = local.with_dtype(torch.float32)
         if method not in self.METHODS:
-            raise ValueError("method must be 'basic' or 'bicgstab'")
+            raise ValueError("method must be 'basic', 'bicgstab' or 'bicgstab_fixed'")
         self.method = method
         self._handle = ctypes.c_void_p()
         _lib.check(_lib.lib().jb_mixed_create(green_op.handle, local.handle, self.green32.handle,
