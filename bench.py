@@ -750,6 +750,88 @@ def run_gradients(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_kernels(args, rank):
+    """Every product entry point once, 3D (128^3) and 2D (1024^2), FP64 and
+    FP32, on fields larger than L2 where the call allows: the launch set an
+    ncu pass reads for per-kernel DRAM traffic and duration.  Prints the list
+    of calls made."""
+    import numpy as np
+    import torch
+
+    import janus_b200.material.elastic.linear.isotropic as material
+    from janus_b200 import _lib
+    from janus_b200 import microstructures as micro
+    from janus_b200 import operators as ops
+    from janus_b200.fft.serial import create_real
+    from janus_b200.gradients import _gradient
+    from janus_b200.green import filtered, truncated, willot2015
+    from janus_b200.solvers import BasicScheme, MixedScheme
+
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    calls = []
+    rng = np.random.default_rng(0)
+    for shape in ((128, 128, 128), (1024, 1024)):
+        dim = len(shape)
+        s = 3 if dim == 2 else 6
+        phase = (rng.random(shape) < 0.3).astype(np.uint8)
+        mat0 = material.create(50.5, 0.3, dim)
+        pars = [(dim * (material.create(g, nu, dim).k - mat0.k), 2 * (g - 50.5))
+                for g, nu in ((1.0, 0.3), (100.0, 0.2))]
+        tens = [ops.isotropic_4(a, b, dim) for a, b in pars]
+        for dt in (torch.float64, torch.float32):
+            tag = "{}D/{}".format(dim, "f64" if dt == torch.float64 else "f32")
+            # FFT objects: r2c / c2r of one scalar field
+            fft = create_real(shape, dtype=dt)
+            x = torch.from_numpy(rng.standard_normal(shape)).to("cuda", dt)
+            c = fft.r2c(x)
+            fft.c2r(c)
+            calls.append(tag + " fft r2c/c2r")
+            # Green operators on two fields (batch), every variant
+            xf = torch.from_numpy(rng.standard_normal((2,) + shape + (s,))).to("cuda", dt)
+            for f in (truncated, filtered, willot2015):
+                g = f(mat0.green_operator(), shape, 1.0, dtype=dt)
+                g.apply_batch(xf)
+                calls.append(tag + " green apply " + f.__name__)
+            g = filtered(mat0.green_operator(), shape, 1.0, dtype=dt)
+            b = torch.from_numpy(rng.integers(0, shape[0], size=(1 << 20, dim)).astype(np.int32))
+            tau = torch.from_numpy(rng.standard_normal((1 << 20, s, 2))).to("cuda", dt)
+            g.apply_by_freq_device(b, tau)
+            calls.append(tag + " green apply_by_freq_device")
+            # local operators: phase map (isotropic, matrices), per-voxel blocks
+            loc = (ops.BlockDiagonalOperator2D if dim == 2 else ops.BlockDiagonalOperator3D
+                   ).from_phases(phase, tens, dtype=dt)
+            y = torch.empty_like(xf)
+            loc.local.apply_device(xf, y, batch=2)
+            mats = np.stack([t.to_memoryview() for t in tens])
+            locm = ops.LocalPhaseOperator(dim, shape, phase, None, None, dt, matrices=mats)
+            locm.apply_device(xf, y, batch=2)
+            a = torch.from_numpy(rng.standard_normal(shape + (s, s))).to("cuda", dt)
+            lin = (ops.BlockDiagonalLinearOperator2D if dim == 2
+                   else ops.BlockDiagonalLinearOperator3D)(a, dtype=dt)
+            lin.apply(xf[0])
+            lin.apply_transpose(xf[0])
+            calls.append(tag + " local (phase, matrices), block linear (+transpose)")
+            # solver steps (local + Green + update + residual), mean stress
+            E = np.eye(s)[:2]
+            sol = BasicScheme(g, loc, nload=2)
+            r = sol.run(E, 2)
+            calls.append(tag + " basic scheme (fill, passes, residual, mean)")
+            if dt == torch.float64:
+                for method in ("basic", "bicgstab"):
+                    MixedScheme(g, loc, nload=2, inner=2, method=method).run(
+                        E, tol=1e-30, max_outer=2)
+                    calls.append(tag + " mixed scheme " + method)
+
+                class _Cell:
+                    pass
+                cell = _Cell()
+                cell.dim, cell.shape, cell.dsph_dmu = dim, shape, 1.0
+                _gradient(cell, r.eps, r.eps.clone())
+                calls.append(tag + " local gradient")
+            torch.cuda.synchronize()
+    print(json.dumps({"workload": "kernels", "calls": calls}), flush=True)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -796,7 +878,7 @@ def main(argv=None):
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the column-schedule autotuner (built-in rules)")
     ap.add_argument("--workload", default="spheres3d",
-                    choices=["spheres3d", "batch2d", "voronoi", "gradients"],
+                    choices=["spheres3d", "batch2d", "voronoi", "gradients", "kernels"],
                     help="spheres3d: the headline step; batch2d: batched 2D cells; "
                          "voronoi: mixed vs FP64 time-to-solution on a 3D Voronoi cell")
     ap.add_argument("--voronoi-n", type=int, default=256)
@@ -849,6 +931,10 @@ def main(argv=None):
     if args.workload == "gradients":
         if rank == 0:
             run_gradients(args, rank)
+        return
+    if args.workload == "kernels":
+        if rank == 0:
+            run_kernels(args, rank)
         return
 
     dist = None

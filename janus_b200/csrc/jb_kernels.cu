@@ -1212,27 +1212,43 @@ bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem, int* nbuf,
   int w = unit == 1 ? 8 : unit * (12 / unit > 0 ? 12 / unit : 1);
   if (tune && tune->w >= unit && tune->w % unit == 0 && tune->w <= 128) w = tune->w;
   if (w < unit) w = unit;
+  // + the axis-0 Green values (4 reals per row, unless tabulated) and alignment
+  auto bytes_for = [&](int ww, int nb) {
+    return n * cs + (nb + 1) * 128 + (nb + 1) * (size_t)n * ww * cs +
+           (stage_ax0 ? (size_t)n * 2 * cs + 128 : 0);
+  };
+  // a TMA box row must span a multiple of 16 bytes: widths that do not
+  // (odd multiples of 3 columns in FP32 2D) are skipped
   for (;; w -= unit) {
-    // + the axis-0 Green values (4 reals per row, unless tabulated) and alignment
-    auto bytes_for = [&](int nb) {
-      return n * cs + (nb + 1) * 128 + (nb + 1) * (size_t)n * w * cs +
-             (stage_ax0 ? (size_t)n * 2 * cs + 128 : 0);
-    };
     // a third input tile for FP32, where two CTAs per SM still fit (measured
     // on B200, 128^3 x 6: FP32 plain passes 8% faster with three; FP64
     // slower, the third tile costing a resident CTA)
     int nb = dtype == F32 ? 3 : 2;
     if (tune && (tune->nbuf == 2 || tune->nbuf == 3)) nb = tune->nbuf;
-    if (bytes_for(nb) > kPipeBudget) nb = 2;
-    const size_t bytes = bytes_for(nb);
-    if (bytes <= kPipeBudget || w <= unit) {
-      if (bytes > kSmemCap - 4096 || (w * cs) % 16 != 0) return false;
+    if (bytes_for(w, nb) > kPipeBudget) nb = 2;
+    const size_t bytes = bytes_for(w, nb);
+    const bool aligned = (w * cs) % 16 == 0;
+    if (aligned && (bytes <= kPipeBudget || w <= unit)) {
+      if (bytes > kSmemCap - 4096) return false;
       *W = w;
       *smem = bytes;
       *nbuf = nb;
       return true;
     }
+    if (w <= unit) break;
   }
+  // no aligned width fits the two-CTA budget (long axes): the narrowest
+  // aligned width, one CTA per SM
+  for (w = unit; w <= 128; w += unit) {
+    if ((w * cs) % 16 != 0) continue;
+    const size_t bytes = bytes_for(w, 2);
+    if (bytes > kSmemCap - 4096) return false;
+    *W = w;
+    *smem = bytes;
+    *nbuf = 2;
+    return true;
+  }
+  return false;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link

@@ -183,3 +183,21 @@ def test_batched_apply_and_fp32():
     y32 = g32.apply(torch.from_numpy(x[0]).float().cuda()).double().cpu().numpy()
     ref = O.green_apply(x[0], MU, NU, 1.0, "filtered")
     assert np.abs(y32 - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(1024, 1024), (512, 384), (768, 256)])
+@pytest.mark.parametrize("variant", ["truncated", "filtered"])
+def test_long_axis_2d_fp32_apply(shape, variant):
+    """2D FP32 grids whose axis-0 tiles need an even column count for the
+    TMA box (the tile-width search skips widths of 24 or 72 bytes)."""
+    import janus_b200.material.elastic.linear.isotropic as _mat
+    from janus_b200.green import filtered as _filtered, truncated as _truncated
+    from oracle import janus_oracle as _O
+    f = _truncated if variant == "truncated" else _filtered
+    g = f(_mat.create(0.75, 0.3, 2).green_operator(), shape, 1.0, dtype=torch.float32)
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal(shape + (3,)).astype(np.float32)
+    y = g.apply(torch.from_numpy(x).cuda()).double().cpu().numpy()
+    ref = _O.green_apply(x.astype(np.float64), 0.75, 0.3, 1.0, variant)
+    assert np.abs(y - ref).max() <= 2e-5 * np.abs(ref).max()
