@@ -890,18 +890,18 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<
   if (threadIdx.x == 0) bulk_wait_read();
 }
 
-template <typename T>
-__global__ void local_kernel(LocalDesc loc, const T* table, int C, int L, int64_t nvox,
-                             const T* x, T* y) {
-  const int64_t total = (int64_t)L * nvox;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t v = i % nvox;
+// y[l][v] = local(v) : x[l][v]; load case l = blockIdx.y; a voxel's CC
+// components move as two-element vectors when CC is even
+template <typename T, int CC>
+__global__ void local_kernel(LocalDesc loc, const T* table, int64_t nvox, const T* x, T* y) {
+  const int64_t off = (int64_t)blockIdx.y * nvox * CC;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox;
+       v += (int64_t)gridDim.x * blockDim.x) {
     const int ph = load_phase(loc.phase, loc.index_bytes, v);
-    T p[6];
-    for (int c = 0; c < C; ++c) p[c] = x[i * C + c];
+    T p[CC];
+    load_voxel<T, CC>(x + off + v * CC, p);
     local_apply<T>(p, table, ph, loc.kind, loc.dim);
-    for (int c = 0; c < C; ++c) y[i * C + c] = p[c];
+    store_voxel<T, CC>(y + off + v * CC, p);
   }
 }
 
@@ -1671,15 +1671,36 @@ cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer, 
 
 cudaError_t launch_local(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,
                          const void* x, void* y, cudaStream_t st) {
-  const int grid = grid_for((int64_t)L * nvox);
-  if (dtype == F64)
-    local_kernel<double><<<grid, kThreads, 0, st>>>(loc, static_cast<const double*>(loc.table),
-                                                    C, L, nvox, static_cast<const double*>(x),
-                                                    static_cast<double*>(y));
-  else
-    local_kernel<float><<<grid, kThreads, 0, st>>>(loc, static_cast<const float*>(loc.table), C,
-                                                   L, nvox, static_cast<const float*>(x),
-                                                   static_cast<float*>(y));
+  if (C != 3 && C != 6) return cudaErrorInvalidValue;
+  const size_t es = dtype == F64 ? 8 : 4;
+  // six-component voxels move as 2-element vectors: the fields must be
+  // aligned to two elements (three-component voxels move element-wise)
+  if (C == 6 && (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % (2 * es) != 0)
+    return cudaErrorInvalidValue;
+  const int g = grid_for(nvox);
+  for (int64_t l0 = 0; l0 < L; l0 += 65535) {  // load cases on grid.y
+    const dim3 grid((unsigned)g, (unsigned)std::min<int64_t>(65535, L - l0));
+    const size_t o = (size_t)l0 * nvox * C * es;
+    const void* xl = static_cast<const char*>(x) + o;
+    void* yl = static_cast<char*>(y) + o;
+    if (dtype == F64) {
+      const double* t = static_cast<const double*>(loc.table);
+      if (C == 6)
+        local_kernel<double, 6><<<grid, kThreads, 0, st>>>(
+            loc, t, nvox, static_cast<const double*>(xl), static_cast<double*>(yl));
+      else
+        local_kernel<double, 3><<<grid, kThreads, 0, st>>>(
+            loc, t, nvox, static_cast<const double*>(xl), static_cast<double*>(yl));
+    } else {
+      const float* t = static_cast<const float*>(loc.table);
+      if (C == 6)
+        local_kernel<float, 6><<<grid, kThreads, 0, st>>>(
+            loc, t, nvox, static_cast<const float*>(xl), static_cast<float*>(yl));
+      else
+        local_kernel<float, 3><<<grid, kThreads, 0, st>>>(
+            loc, t, nvox, static_cast<const float*>(xl), static_cast<float*>(yl));
+    }
+  }
   return cudaGetLastError();
 }
 
