@@ -1015,12 +1015,6 @@ __global__ void axpy_f32_to_f64_kernel(int64_t n, const float* __restrict__ d,
     y[i] += d[i];
 }
 
-__global__ void convert_f64_to_f32_kernel(int64_t n, const double* __restrict__ x,
-                                          float* __restrict__ y) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    y[i] = static_cast<float>(x[i]);
-}
 
 template <typename T, int DIM>
 __global__ void green_table_kernel(GreenTables<T> gt, int64_t n0, int64_t n1, int64_t m_last,
@@ -1813,11 +1807,6 @@ cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStr
                    (reinterpret_cast<uintptr_t>(y) & 15u) == 0;
   if (!vec) return cudaErrorInvalidValue;
   axpy_f32_to_f64_kernel<<<grid_for(n / 4 + 1), kThreads, 0, st>>>(n, d, y);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_convert_f64_to_f32(int64_t n, const double* x, float* y, cudaStream_t st) {
-  convert_f64_to_f32_kernel<<<grid_for(n), kThreads, 0, st>>>(n, x, y);
   return cudaGetLastError();
 }
 

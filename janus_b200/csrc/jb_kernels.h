@@ -85,8 +85,6 @@ cudaError_t launch_krylov_update(int dtype, int which, int64_t nel, int L, void*
 
 // y[i] += (double) d[i] over n elements (FP64 field, FP32 correction)
 cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStream_t st);
-// y[i] = (float) x[i]
-cudaError_t launch_convert_f64_to_f32(int64_t n, const double* x, float* y, cudaStream_t st);
 
 int max_axis_length(int dtype);
 // bit 0: a kernel gave up a bounded wait (see jb_async.cuh); cleared on read
