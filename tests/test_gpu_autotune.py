@@ -23,7 +23,11 @@ def _green(dim, n, variant, dtype):
                                          (2, 64, torch.float64), (2, 96, torch.float32),
                                          (2, 256, torch.float64),
                                          (3, (256, 16, 16), torch.float64),
-                                         (3, (256, 16, 16), torch.float32)])
+                                         (3, (256, 16, 16), torch.float32),
+                                         (3, (128, 16, 16), torch.float64),
+                                         (3, (128, 16, 16), torch.float32),
+                                         (2, (128, 64), torch.float64),
+                                         (2, (128, 62), torch.float32)])
 def test_every_candidate_computes_the_same_operator(dim, n, dtype):
     g = _green(dim, n, "filtered", dtype)
     s = g.ishape[-1]
