@@ -225,6 +225,29 @@ int jb_solver_set_load(jb_solver *solver, const double *E);
  * double[nload], may be NULL). */
 int jb_solver_step(jb_solver *solver, void *eps, double *res_dev,
                    void *stream);
+/* ---- restarted GMRES(m) ------------------------------------------------- */
+
+/* Replaces the reference's Krylov usage, scipy's gmres over a LinearOperator
+ * whose matvec is x + Gamma0[(C - C0):x]
+ * (examples/square_inclusion_scipy.py:52-59, 88), for `nload` load cases at
+ * once (one Krylov space each), FP64 only, basis of restart + 1 fields kept
+ * on the device.  The handles are borrowed and must outlive the solver. */
+typedef struct jb_gmres_s jb_gmres;
+int jb_gmres_create(jb_green *green, jb_local *local, int nload, int restart,
+                    jb_gmres **out);
+int jb_gmres_destroy(jb_gmres *solver);
+/* Solves (I + Gamma0 (C - C0)) eps = E from eps (set to E first if init).
+ * Stops when every load case has ||E - eps - Gamma0[(C - C0):eps]|| /
+ * (sqrt(N) ||E||) <= tol (the basic scheme's residual measure), checked on
+ * the true residual at each restart, or after max_iter Arnoldi steps.
+ * residuals: host double[max_iter][nload], the Givens estimate of each step
+ * (may be NULL); iters_out: Arnoldi steps done; final_residuals: host
+ * double[nload], the true residual at exit (may be NULL); mean_tau as for
+ * jb_solver_run.  Returns after the work on `stream` has completed. */
+int jb_gmres_run(jb_gmres *solver, const double *E, void *eps, int init,
+                 int max_iter, double tol, double *residuals, int *iters_out,
+                 double *final_residuals, double *mean_tau, void *stream);
+
 /* ---- mixed-precision basic scheme (defect correction) ------------------- */
 
 /* No counterpart in the reference (its solver loop is FP64 only).  Solves the

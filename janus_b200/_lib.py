@@ -85,6 +85,10 @@ _SIGS = {
     "jb_mixed_create": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int,
                          ctypes.POINTER(c_void_p)], c_int),
     "jb_mixed_destroy": ([c_void_p], c_int),
+    "jb_gmres_create": ([c_void_p, c_void_p, c_int, c_int, ctypes.POINTER(c_void_p)], c_int),
+    "jb_gmres_destroy": ([c_void_p], c_int),
+    "jb_gmres_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_double, P_double, P_int,
+                      P_double, P_double, c_void_p], c_int),
     "jb_mixed_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_int, c_double, P_double,
                       P_int, P_int, P_double, c_void_p], c_int),
 }

@@ -84,6 +84,22 @@ cudaError_t launch_krylov_update(int dtype, int which, int64_t nel, int L, void*
                                  const KrylovState* state, double* partials, cudaStream_t st);
 
 // y[i] += (double) d[i] over n elements (FP64 field, FP32 correction)
+// GMRES(m) vector kernels (FP64, batched over L load cases; basis vector i of
+// load case l at V + i * vs + l * nel; at most gmres_chunk() vectors a launch)
+int gmres_chunk();
+// out[l * ldo + o0 + i] = w . V_{j0+i}, i < cnt (partials: L * chunk * blocks)
+cudaError_t launch_gmres_dots(int64_t nel, int L, const double* w, const double* V, int64_t vs,
+                              int j0, int cnt, double* partials, double* out, int ldo, int o0,
+                              cudaStream_t st);
+// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}
+cudaError_t launch_gmres_axpys(int64_t nel, int L, double* w, const double* V, int64_t vs, int j0,
+                               int cnt, const double* coef, int ldc, int c0, double sign,
+                               cudaStream_t st);
+// w /= sqrt(sq[l]) (0 where the norm is 0 or not finite)
+cudaError_t launch_gmres_scale(int64_t nel, int L, double* w, const double* sq, cudaStream_t st);
+// r[l][v][c] = E[l][c] - ax[l][v][c] (r may alias ax)
+cudaError_t launch_gmres_resid(int64_t nvox, int C, int L, const double* E, const double* ax,
+                               double* r, cudaStream_t st);
 cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStream_t st);
 
 int max_axis_length(int dtype);

@@ -261,6 +261,103 @@ __global__ void __launch_bounds__(kKrThreads)
   if (threadIdx.x == 0) partials[((int64_t)l * 2) * nb + blockIdx.x] = acc;
 }
 
+// ---------------------------------------------------------------------------
+// GMRES(m) vector kernels (FP64).  Basis vector i of load case l starts at
+// V + i * vs + l * nel; up to kGmChunk basis vectors are streamed per launch
+// next to the vector w they are combined with.
+// ---------------------------------------------------------------------------
+constexpr int kGmChunk = 8;
+
+// partials[(l * kGmChunk + i) * nb + b] = block b's share of w . V_{j0+i}
+__global__ void __launch_bounds__(kKrThreads)
+    gm_dots_kernel(int64_t nel, const double* __restrict__ w, const double* __restrict__ V,
+                   int64_t vs, int j0, int cnt, double* partials) {
+  __shared__ double red[kKrThreads / 32];
+  const int l = blockIdx.y, nb = gridDim.x;
+  const int64_t off = (int64_t)l * nel;
+  const double* wl = w + off;
+  const double* vb = V + (int64_t)j0 * vs + off;
+  double acc[kGmChunk];
+#pragma unroll
+  for (int i = 0; i < kGmChunk; ++i) acc[i] = 0.0;
+  const int64_t stride = (int64_t)nb * blockDim.x;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride) {
+    const double x = wl[e];
+#pragma unroll
+    for (int i = 0; i < kGmChunk; ++i)
+      if (i < cnt) acc[i] += x * vb[(int64_t)i * vs + e];
+  }
+#pragma unroll
+  for (int i = 0; i < kGmChunk; ++i) {
+    if (i < cnt) {  // cnt is uniform over the block
+      const double t = kr_block_sum(acc[i], red);
+      if (threadIdx.x == 0) partials[((int64_t)l * kGmChunk + i) * nb + blockIdx.x] = t;
+    }
+  }
+}
+
+// out[l * ldo + o0 + i] = sum_b partials[(l * kGmChunk + i) * nb + b], fixed order
+__global__ void __launch_bounds__(kKrThreads)
+    gm_reduce_kernel(const double* partials, int nb, double* out, int ldo, int o0) {
+  __shared__ double red[kKrThreads / 32];
+  const int i = blockIdx.x, l = blockIdx.y;
+  double t = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    t += partials[((int64_t)l * kGmChunk + i) * nb + b];
+  t = kr_block_sum(t, red);
+  if (threadIdx.x == 0) out[(int64_t)l * ldo + o0 + i] = t;
+}
+
+// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}
+__global__ void __launch_bounds__(kKrThreads)
+    gm_axpys_kernel(int64_t nel, double* __restrict__ w, const double* __restrict__ V,
+                    int64_t vs, int j0, int cnt, const double* __restrict__ coef, int ldc,
+                    int c0, double sign) {
+  const int l = blockIdx.y;
+  const int64_t off = (int64_t)l * nel;
+  double* wl = w + off;
+  const double* vb = V + (int64_t)j0 * vs + off;
+  double a[kGmChunk];
+#pragma unroll
+  for (int i = 0; i < kGmChunk; ++i) a[i] = i < cnt ? sign * coef[(int64_t)l * ldc + c0 + i] : 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride) {
+    double x = wl[e];
+#pragma unroll
+    for (int i = 0; i < kGmChunk; ++i)
+      if (i < cnt) x += a[i] * vb[(int64_t)i * vs + e];
+    wl[e] = x;
+  }
+}
+
+// w /= sqrt(sq[l]); a vector of zero or non-finite norm becomes 0 (the
+// Arnoldi process of that load case has broken down or converged)
+__global__ void __launch_bounds__(kKrThreads)
+    gm_scale_kernel(int64_t nel, double* __restrict__ w, const double* __restrict__ sq) {
+  const int l = blockIdx.y;
+  const double n = sqrt(sq[l]);
+  const double f = (n > 0.0 && isfinite(1.0 / n)) ? 1.0 / n : 0.0;
+  double* wl = w + (int64_t)l * nel;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride)
+    wl[e] *= f;
+}
+
+// r = E_l - ax (the residual of the macroscopic load; r may alias ax)
+template <int C>
+__global__ void __launch_bounds__(kKrThreads)
+    gm_resid_kernel(int64_t nvox, const double* __restrict__ E, const double* ax, double* r) {
+  const int l = blockIdx.y;
+  const int64_t off = (int64_t)l * nvox * C;
+  double e[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) e[c] = E[l * C + c];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += stride)
+#pragma unroll
+    for (int c = 0; c < C; ++c) r[off + v * C + c] = e[c] - ax[off + v * C + c];
+}
+
 int kr_blocks(int64_t nel, int L) {
   int64_t b = (nel + kKrThreads * 4 - 1) / (kKrThreads * 4);
   const int64_t cap = (148 * 8 + L - 1) / L;
@@ -272,6 +369,47 @@ int kr_blocks(int64_t nel, int L) {
 }  // namespace
 
 int krylov_blocks(int64_t nel, int L) { return kr_blocks(nel, L); }
+
+int gmres_chunk() { return kGmChunk; }
+
+cudaError_t launch_gmres_dots(int64_t nel, int L, const double* w, const double* V, int64_t vs,
+                              int j0, int cnt, double* partials, double* out, int ldo, int o0,
+                              cudaStream_t st) {
+  if (cnt < 1 || cnt > kGmChunk) return cudaErrorInvalidValue;
+  const int nb = kr_blocks(nel, L);
+  gm_dots_kernel<<<dim3((unsigned)nb, (unsigned)L), kKrThreads, 0, st>>>(nel, w, V, vs, j0, cnt,
+                                                                          partials);
+  gm_reduce_kernel<<<dim3((unsigned)cnt, (unsigned)L), kKrThreads, 0, st>>>(partials, nb, out,
+                                                                             ldo, o0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gmres_axpys(int64_t nel, int L, double* w, const double* V, int64_t vs, int j0,
+                               int cnt, const double* coef, int ldc, int c0, double sign,
+                               cudaStream_t st) {
+  if (cnt < 1 || cnt > kGmChunk) return cudaErrorInvalidValue;
+  gm_axpys_kernel<<<dim3((unsigned)kr_blocks(nel, L), (unsigned)L), kKrThreads, 0, st>>>(
+      nel, w, V, vs, j0, cnt, coef, ldc, c0, sign);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gmres_scale(int64_t nel, int L, double* w, const double* sq, cudaStream_t st) {
+  gm_scale_kernel<<<dim3((unsigned)kr_blocks(nel, L), (unsigned)L), kKrThreads, 0, st>>>(nel, w,
+                                                                                         sq);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gmres_resid(int64_t nvox, int C, int L, const double* E, const double* ax,
+                               double* r, cudaStream_t st) {
+  const dim3 grid((unsigned)kr_blocks(nvox * C, L), (unsigned)L);
+  if (C == 3)
+    gm_resid_kernel<3><<<grid, kKrThreads, 0, st>>>(nvox, E, ax, r);
+  else if (C == 6)
+    gm_resid_kernel<6><<<grid, kKrThreads, 0, st>>>(nvox, E, ax, r);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_krylov_dot(int dtype, int64_t nel, int L, const void* a, const void* b,
                               const void* c, const void* d, double* partials, cudaStream_t st) {

@@ -245,3 +245,122 @@ class MixedScheme:
         n = outer.value
         return MixedResult(eps=eps, residuals=res[:n].copy(), outer_iterations=n,
                            fp32_iterations=fp32.value, mean_tau=mean)
+
+
+@dataclass
+class GMRESResult:
+    eps: torch.Tensor          # (nload,) + grid + (s,), FP64 on the device
+    residuals: np.ndarray      # (iterations, nload): Givens estimate after each Arnoldi step
+    final_residuals: np.ndarray  # (nload,): true residual at exit
+    iterations: int            # Arnoldi steps (operator applications besides restarts)
+    mean_tau: np.ndarray       # (nload, s)
+
+    def mean_stress(self, mat0, avg_eps):
+        return _c0_apply(mat0, np.atleast_2d(avg_eps)) + self.mean_tau
+
+
+class GMRES:
+    """Restarted GMRES(``restart``) on (I + Gamma0 (C - C0)) eps = E, FP64,
+    with the Krylov basis on the device: the reference's Krylov route,
+    examples/square_inclusion_scipy.py:52-59, 88, which hands this operator
+    to scipy's gmres.  Every load case (rows of E) has its own Krylov space;
+    the stopping test is the basic scheme's residual ||E - A eps|| /
+    (sqrt(N) ||E||) <= tol, checked on the true residual at each restart.
+    The basis holds restart + 1 fields of nload x grid x s doubles."""
+
+    def __init__(self, green_op, local_op, nload=1, restart=20):
+        if isinstance(local_op, _BlockDiagonalOperator):
+            local = local_op.local
+        else:
+            local = local_op
+        if not isinstance(local, LocalPhaseOperator):
+            raise ValueError("the solver needs phase-map or field local operators")
+        if green_op.dtype != torch.float64 or local.dtype != torch.float64:
+            raise ValueError("GMRES takes FP64 operators")
+        if tuple(local.shape) != tuple(green_op.ishape[:-1]):
+            raise ValueError("local and green operators must share the grid")
+        self.green_op = green_op
+        self.local = local
+        self.nload = int(nload)
+        self.restart = int(restart)
+        self._handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().jb_gmres_create(green_op.handle, local.handle, self.nload,
+                                              self.restart, ctypes.byref(self._handle)))
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().jb_gmres_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    @property
+    def field_shape(self):
+        return (self.nload,) + tuple(self.green_op.ishape)
+
+    def run(self, avg_eps, tol=1e-8, max_iter=1000, eps=None, init=None):
+        """eps (device FP64 tensor of field_shape) is the initial guess and is
+        updated in place; if omitted, a new field set to E is used."""
+        E = np.ascontiguousarray(np.asarray(avg_eps, dtype=np.float64).reshape(
+            self.nload, self.green_op.ishape[-1]))
+        if eps is None:
+            eps = torch.empty(self.field_shape, dtype=torch.float64, device=A.device())
+            init = True if init is None else init
+        elif tuple(eps.shape) != self.field_shape or eps.dtype != torch.float64 or \
+                not eps.is_contiguous() or eps.device.type != "cuda":
+            raise ValueError("eps must be a contiguous FP64 CUDA tensor of shape {0}".format(
+                self.field_shape))
+        res = np.zeros((max(int(max_iter), 1), self.nload))
+        final = np.zeros(self.nload)
+        it = ctypes.c_int(0)
+        mean = np.zeros((self.nload, self.green_op.ishape[-1]))
+        P = ctypes.POINTER(ctypes.c_double)
+        _lib.check(_lib.lib().jb_gmres_run(
+            self._handle, E.ctypes.data_as(P), ctypes.c_void_p(eps.data_ptr()),
+            int(bool(init)), int(max_iter), float(tol), res.ctypes.data_as(P),
+            ctypes.byref(it), final.ctypes.data_as(P), mean.ctypes.data_as(P),
+            ctypes.c_void_p(A.stream_handle())))
+        n = it.value
+        return GMRESResult(eps=eps, residuals=res[:n].copy(), final_residuals=final,
+                           iterations=n, mean_tau=mean)
+
+
+class LippmannSchwingerOperator:
+    """x -> x + Gamma0[(C - C0):x] on flattened host vectors (FP64), the
+    matvec of the reference's examples/square_inclusion_scipy.py:52-59
+    (``rmatvec``: x + (C - C0):Gamma0[x]), evaluated on the GPU; hand it to
+    ``scipy.sparse.linalg.aslinearoperator`` and scipy's Krylov solvers."""
+
+    def __init__(self, green_op, local_op):
+        local = local_op.local if isinstance(local_op, _BlockDiagonalOperator) else local_op
+        if not isinstance(local, LocalPhaseOperator):
+            raise ValueError("the operator needs phase-map or field local operators")
+        if green_op.dtype != torch.float64 or local.dtype != torch.float64:
+            raise ValueError("LippmannSchwingerOperator takes FP64 operators")
+        self.green_op = green_op
+        self.local = local
+        self.grid_shape = tuple(green_op.ishape)
+        n = int(np.prod(self.grid_shape))
+        self.shape = (n, n)
+        self.dtype = np.dtype(np.float64)
+
+    def _dev(self, x):
+        return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64).reshape(
+            self.grid_shape)).to(A.device())
+
+    def matvec(self, x):
+        xd = self._dev(x)
+        t = torch.empty_like(xd)
+        self.local.apply_device(xd, t)
+        self.green_op._apply_device(t, t)
+        return (xd + t).cpu().numpy().reshape(np.shape(x))
+
+    def rmatvec(self, x):
+        xd = self._dev(x)
+        g = torch.empty_like(xd)
+        self.green_op._apply_device(xd, g)
+        t = torch.empty_like(xd)
+        self.local.apply_device(g, t)
+        return (xd + t).cpu().numpy().reshape(np.shape(x))
