@@ -437,6 +437,26 @@ def run_gpu(args, rank, world, dist):
                 "C_eff_max_rel_diff_vs_fp64": float(np.abs(ck - c64).max() / np.abs(c64).max())}
             solve["mixed_bicgstab_speedup"] = round(
                 solve["fp64"]["seconds"] / solve["mixed_bicgstab"]["seconds"], 3)
+            # FP64 restarted GMRES over the same operator (the reference
+            # examples' Krylov route), same stopping test
+            from janus_b200.solvers import GMRES
+            gm = GMRES(green, loc, nload=6, restart=args.gmres_restart)
+            eps4 = torch.empty_like(eps2)
+            gm.run(E, tol=1e-30, max_iter=2, eps=eps4, init=True)  # warm the kernels
+            torch.cuda.synchronize()
+            a.record()
+            rg = gm.run(E, tol=args.tol, max_iter=args.solve_max_iter, eps=eps4, init=True)
+            b.record()
+            torch.cuda.synchronize()
+            cg = rg.mean_stress(mat0, E)
+            solve["gmres_fp64"] = {
+                "restart": args.gmres_restart, "arnoldi_steps": rg.iterations,
+                "seconds": round(a.elapsed_time(b) / 1e3, 4),
+                "final_residual_max": float(rg.final_residuals.max()),
+                "C_eff_max_rel_diff_vs_fp64": float(np.abs(cg - c64).max() / np.abs(c64).max())}
+            solve["gmres_fp64_speedup"] = round(
+                solve["fp64"]["seconds"] / solve["gmres_fp64"]["seconds"], 3)
+            del gm
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -574,7 +594,7 @@ def run_voronoi(args, rank):
     from janus_b200 import microstructures as micro
     from janus_b200 import operators as ops
     from janus_b200.green import filtered, truncated
-    from janus_b200.solvers import BasicScheme, MixedScheme
+    from janus_b200.solvers import GMRES, BasicScheme, MixedScheme
 
     torch.cuda.set_device(env_int("LOCAL_RANK", 0))
     n = args.voronoi_n
@@ -643,7 +663,22 @@ def run_voronoi(args, rank):
             "final_residual_max": float(rk.residuals[-1].max()),
             "C_eff_max_rel_diff_vs_fp64": float(np.abs(ck - c64).max() / np.abs(c64).max())}
         out[name]["speedup_bicgstab"] = round(t64 / tk, 3)
-        del kry, green
+        del kry
+        gm = GMRES(green, loc, nload=len(E), restart=args.gmres_restart)
+        gm.run(E, tol=1e-30, max_iter=2)  # warm
+        torch.cuda.synchronize()
+        a.record()
+        rg = gm.run(E, tol=args.tol, max_iter=args.solve_max_iter * args.inner)
+        b.record()
+        torch.cuda.synchronize()
+        tg = a.elapsed_time(b) / 1e3
+        cg = rg.mean_stress(mat0, E)
+        out[name]["gmres_fp64"] = {
+            "restart": args.gmres_restart, "arnoldi_steps": rg.iterations,
+            "seconds": round(tg, 3), "final_residual_max": float(rg.final_residuals.max()),
+            "C_eff_max_rel_diff_vs_fp64": float(np.abs(cg - c64).max() / np.abs(c64).max())}
+        out[name]["speedup_gmres_fp64"] = round(t64 / tg, 3)
+        del gm, green
         torch.cuda.empty_cache()
     clocks = sampler.stop()
     line = {"metric": "time-to-solution, mixed (FP32 + FP64 defect correction) vs FP64",
@@ -898,6 +933,8 @@ def main(argv=None):
     ap.add_argument("--batch-branches", type=int, default=8)
     ap.add_argument("--inner-method", default="basic", choices=["basic", "bicgstab"],
                     help="inner solver of the batched mixed scheme")
+    ap.add_argument("--gmres-restart", type=int, default=20,
+                    help="restart length of the FP64 GMRES time-to-solution leg")
     ap.add_argument("--krylov-inner", type=int, default=25,
                     help="BiCGSTAB iterations per defect-correction step")
     # internal: CPU worker process

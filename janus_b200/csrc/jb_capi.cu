@@ -1210,9 +1210,13 @@ int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_it
 // (examples/square_inclusion_scipy.py:52-59, 88).  Here the operator is one
 // fused pass sequence (rhs epilogue: out = in + Gamma0[(C - C0):in]) and the
 // Krylov vectors stay on the device, one Krylov space per load case.  The
-// Arnoldi basis is orthogonalised by classical Gram-Schmidt with one
-// reorthogonalisation (two projection sweeps, each streaming up to 8 basis
-// vectors per launch); the small Hessenberg least-squares problems (Givens
+// Arnoldi process runs on K = Gamma0 (C - C0) (same Krylov spaces as A,
+// H_A = H_K + I).  Its basis is orthogonalised by classical Gram-Schmidt (each projection
+// sweep one pass of dot products and one of updates, up to 8 basis vectors
+// streamed per launch, |w|^2 computed with the former and |w'|^2 with the
+// latter) and swept a second time only when the first sweep cancelled more
+// than half of |w|^2 (|w'| < |w| / sqrt(2), the "twice is enough" test of
+// Kahan and Parlett); the small Hessenberg least-squares problems (Givens
 // rotations) are solved on the host.  Residuals are relative to
 // sqrt(N) |E_l|, the normalisation of the basic scheme's residual
 // (square_basic.py:86): for the basic scheme's iterate eps_k, E - A eps_k is
@@ -1329,6 +1333,8 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
   JB_CUDA(cudaMemcpyAsync(Ed, E, sizeof(double) * L * C, cudaMemcpyHostToDevice, st));
   if (init)
     JB_TRY(launch_status(jb::launch_fill_macro(F64, C, L, nvox, Ed, eps, st), "fill"));
+  std::vector<double> H((size_t)L * (m + 1) * m), cs((size_t)L * m), sn((size_t)L * m),
+      g((size_t)L * (m + 1)), hh((size_t)L * ldh), sq(L), beta(L), rel(L), yh((size_t)L * m);
   jb::LocalDesc loc = local_desc(S->local);
   auto apply = [&](const double* in, double* o) {  // o = in + Gamma0[(C - C0):in]
     jb::UpdateDesc u;
@@ -1337,30 +1343,41 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     u.rhs = in;
     return green_passes(G, in, o, L, S->spec.p, &loc, &u, nullptr, st);
   };
+  // the Arnoldi process runs on K = Gamma0 (C - C0), whose Krylov spaces are
+  // those of A = I + K (H_A = H_K + I): w = K v has no component along v from
+  // the identity for the projection to cancel
+  auto applyK = [&](const double* in, double* o) {
+    return green_passes(G, in, o, L, S->spec.p, &loc, nullptr, nullptr, st);
+  };
   auto norm2 = [&](const double* w) {  // sq[l] = w . w on the device
     return launch_status(jb::launch_gmres_dots(nel, L, w, w, 0, 0, 1, part, sqd, 1, 0, st),
                          "gmres_dots");
   };
-  // w -= sum_{i <= j} (V_i . w) V_i, twice; coefficients of sweep q at h[l][q (m+1) + i]
-  auto orthogonalise = [&](double* w, int j) {
-    for (int q = 0; q < 2; ++q) {
-      for (int i0 = 0; i0 <= j; i0 += ch) {
-        const int cnt = std::min(ch, j + 1 - i0);
-        JB_TRY(launch_status(
-            jb::launch_gmres_dots(nel, L, w, V, vs, i0, cnt, part, hd, ldh, q * (m + 1) + i0, st),
-            "gmres_dots"));
-      }
-      for (int i0 = 0; i0 <= j; i0 += ch) {
-        const int cnt = std::min(ch, j + 1 - i0);
-        JB_TRY(launch_status(jb::launch_gmres_axpys(nel, L, w, V, vs, i0, cnt, hd, ldh,
-                                                    q * (m + 1) + i0, -1.0, st),
-                             "gmres_axpys"));
-      }
+  // one sweep q on w = V_{j+1}: h[l][q (m+1) + i] = V_i . w for i <= j (sweep 0
+  // also w . w at i = j + 1), then w -= sum_{i <= j} h_i V_i and sq = |w|^2
+  auto sweep = [&](int j, int q) {
+    double* w = V + (int64_t)(j + 1) * vs;
+    const int nd = q == 0 ? j + 2 : j + 1;
+    for (int i0 = 0; i0 < nd; i0 += ch) {
+      const int cnt = std::min(ch, nd - i0);
+      JB_TRY(launch_status(
+          jb::launch_gmres_dots(nel, L, w, V, vs, i0, cnt, part, hd, ldh, q * (m + 1) + i0, st),
+          "gmres_dots"));
     }
+    for (int i0 = 0; i0 <= j; i0 += ch) {
+      const int cnt = std::min(ch, j + 1 - i0);
+      const bool last = i0 + cnt > j;
+      JB_TRY(launch_status(jb::launch_gmres_axpys(nel, L, w, V, vs, i0, cnt, hd, ldh,
+                                                  q * (m + 1) + i0, -1.0, last ? part : nullptr,
+                                                  last ? sqd : nullptr, st),
+                           "gmres_axpys"));
+    }
+    JB_CUDA(cudaMemcpyAsync(hh.data() + (size_t)0, hd, sizeof(double) * L * ldh,
+                            cudaMemcpyDeviceToHost, st));
+    JB_CUDA(cudaMemcpyAsync(sq.data(), sqd, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
+    JB_CUDA(cudaStreamSynchronize(st));
     return JB_OK;
   };
-  std::vector<double> H((size_t)L * (m + 1) * m), cs((size_t)L * m), sn((size_t)L * m),
-      g((size_t)L * (m + 1)), hh((size_t)L * ldh), sq(L), beta(L), rel(L), yh((size_t)L * m);
   std::vector<int> active(L), kuse(L);
   int it = 0;
   for (;;) {
@@ -1389,14 +1406,18 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     int j = 0;
     for (; j < m && it < max_iter; ++j, ++it) {
       double* w = V + (int64_t)(j + 1) * vs;
-      JB_TRY(apply(V + (int64_t)j * vs, w));
-      JB_TRY(orthogonalise(w, j));
-      JB_TRY(norm2(w));
+      JB_TRY(applyK(V + (int64_t)j * vs, w));
+      JB_TRY(sweep(j, 0));
+      bool again = false;
+      for (int l = 0; l < L; ++l)
+        if (active[l] && sq[l] < 0.5 * hh[(size_t)l * ldh + j + 1]) again = true;
+      if (again) {
+        JB_TRY(sweep(j, 1));
+      } else {
+        for (int l = 0; l < L; ++l)
+          for (int i = 0; i <= j; ++i) hh[(size_t)l * ldh + (m + 1) + i] = 0.0;
+      }
       JB_TRY(launch_status(jb::launch_gmres_scale(nel, L, w, sqd, st), "gmres_scale"));
-      JB_CUDA(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * L * ldh, cudaMemcpyDeviceToHost,
-                              st));
-      JB_CUDA(cudaMemcpyAsync(sq.data(), sqd, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
-      JB_CUDA(cudaStreamSynchronize(st));
       bool any = false;
       for (int l = 0; l < L; ++l) {
         double* Hl = &H[(size_t)l * (m + 1) * m];  // column-major (m + 1) x m
@@ -1408,6 +1429,7 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
         double* col = Hl + (size_t)j * (m + 1);
         for (int i = 0; i <= j; ++i)
           col[i] = hh[(size_t)l * ldh + i] + hh[(size_t)l * ldh + (m + 1) + i];
+        col[j] += 1.0;  // H_A = H_K + I
         const double hn = std::sqrt(sq[l]);
         col[j + 1] = hn;
         for (int i = 0; i < j; ++i) {  // earlier rotations
@@ -1457,7 +1479,8 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     JB_CUDA(cudaMemcpyAsync(yd, yh.data(), sizeof(double) * L * m, cudaMemcpyHostToDevice, st));
     for (int i0 = 0; i0 < kmax; i0 += ch) {
       const int cnt = std::min(ch, kmax - i0);
-      JB_TRY(launch_status(jb::launch_gmres_axpys(nel, L, x, V, vs, i0, cnt, yd, m, i0, 1.0, st),
+      JB_TRY(launch_status(jb::launch_gmres_axpys(nel, L, x, V, vs, i0, cnt, yd, m, i0, 1.0,
+                                                    nullptr, nullptr, st),
                            "gmres_axpys"));
     }
   }

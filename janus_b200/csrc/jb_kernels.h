@@ -91,10 +91,11 @@ int gmres_chunk();
 cudaError_t launch_gmres_dots(int64_t nel, int L, const double* w, const double* V, int64_t vs,
                               int j0, int cnt, double* partials, double* out, int ldo, int o0,
                               cudaStream_t st);
-// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}
+// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}; with partials
+// and sq (both or neither), sq[l] = |w|^2 after the update
 cudaError_t launch_gmres_axpys(int64_t nel, int L, double* w, const double* V, int64_t vs, int j0,
                                int cnt, const double* coef, int ldc, int c0, double sign,
-                               cudaStream_t st);
+                               double* partials, double* sq, cudaStream_t st);
 // w /= sqrt(sq[l]) (0 where the norm is 0 or not finite)
 cudaError_t launch_gmres_scale(int64_t nel, int L, double* w, const double* sq, cudaStream_t st);
 // r[l][v][c] = E[l][c] - ax[l][v][c] (r may alias ax)

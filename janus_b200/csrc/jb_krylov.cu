@@ -308,11 +308,13 @@ __global__ void __launch_bounds__(kKrThreads)
   if (threadIdx.x == 0) out[(int64_t)l * ldo + o0 + i] = t;
 }
 
-// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}
+// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}; with partials,
+// also block b's share of |w|^2 after the update at partials[l * kGmChunk * nb + b]
 __global__ void __launch_bounds__(kKrThreads)
     gm_axpys_kernel(int64_t nel, double* __restrict__ w, const double* __restrict__ V,
                     int64_t vs, int j0, int cnt, const double* __restrict__ coef, int ldc,
-                    int c0, double sign) {
+                    int c0, double sign, double* partials) {
+  __shared__ double red[kKrThreads / 32];
   const int l = blockIdx.y;
   const int64_t off = (int64_t)l * nel;
   double* wl = w + off;
@@ -321,12 +323,18 @@ __global__ void __launch_bounds__(kKrThreads)
 #pragma unroll
   for (int i = 0; i < kGmChunk; ++i) a[i] = i < cnt ? sign * coef[(int64_t)l * ldc + c0 + i] : 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double nn = 0.0;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride) {
     double x = wl[e];
 #pragma unroll
     for (int i = 0; i < kGmChunk; ++i)
       if (i < cnt) x += a[i] * vb[(int64_t)i * vs + e];
     wl[e] = x;
+    nn += x * x;
+  }
+  if (partials) {  // uniform over the grid
+    nn = kr_block_sum(nn, red);
+    if (threadIdx.x == 0) partials[(int64_t)l * kGmChunk * gridDim.x + blockIdx.x] = nn;
   }
 }
 
@@ -386,10 +394,14 @@ cudaError_t launch_gmres_dots(int64_t nel, int L, const double* w, const double*
 
 cudaError_t launch_gmres_axpys(int64_t nel, int L, double* w, const double* V, int64_t vs, int j0,
                                int cnt, const double* coef, int ldc, int c0, double sign,
-                               cudaStream_t st) {
+                               double* partials, double* sq, cudaStream_t st) {
   if (cnt < 1 || cnt > kGmChunk) return cudaErrorInvalidValue;
-  gm_axpys_kernel<<<dim3((unsigned)kr_blocks(nel, L), (unsigned)L), kKrThreads, 0, st>>>(
-      nel, w, V, vs, j0, cnt, coef, ldc, c0, sign);
+  if ((partials == nullptr) != (sq == nullptr)) return cudaErrorInvalidValue;
+  const int nb = kr_blocks(nel, L);
+  gm_axpys_kernel<<<dim3((unsigned)nb, (unsigned)L), kKrThreads, 0, st>>>(
+      nel, w, V, vs, j0, cnt, coef, ldc, c0, sign, partials);
+  if (sq)
+    gm_reduce_kernel<<<dim3(1u, (unsigned)L), kKrThreads, 0, st>>>(partials, nb, sq, 1, 0);
   return cudaGetLastError();
 }
 
