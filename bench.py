@@ -356,25 +356,34 @@ def run_gpu(args, rank, world, dist):
     e2e = None
     if not args.no_e2e:
         out = torch.empty(solver.field_shape, dtype=dtype, pin_memory=True)
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        t0 = time.perf_counter()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record()
-        loc2 = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dtype)
-        sol2 = BasicScheme(green, loc2, nload=6)
-        t1 = time.perf_counter()
-        r = sol2.run(E, args.steps)
-        t2 = time.perf_counter()
-        out.copy_(r.eps, non_blocking=True)
-        s1.record()
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        parts = {"setup_ms": round((t1 - t0) * 1e3, 2), "solve_ms": round((t2 - t1) * 1e3, 2),
-                 "copy_out_ms": round((time.perf_counter() - t2) * 1e3, 2)}
-        e2e_ms = max(s0.elapsed_time(s1), wall * 1e3)
+        # three repetitions, the median reported (each one complete: operators
+        # built from the host phase map, K iterations, field copied out)
+        reps = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            t0 = time.perf_counter()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record()
+            loc2 = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dtype)
+            sol2 = BasicScheme(green, loc2, nload=6)
+            t1 = time.perf_counter()
+            r = sol2.run(E, args.steps)
+            t2 = time.perf_counter()
+            out.copy_(r.eps, non_blocking=True)
+            s1.record()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            reps.append((max(s0.elapsed_time(s1), wall * 1e3),
+                         {"setup_ms": round((t1 - t0) * 1e3, 2),
+                          "solve_ms": round((t2 - t1) * 1e3, 2),
+                          "copy_out_ms": round((time.perf_counter() - t2) * 1e3, 2)}))
+            del r, sol2, loc2
+        reps_sorted = sorted(reps, key=lambda x: x[0])
+        e2e_ms, parts = reps_sorted[1]
+        parts = dict(parts, repetitions_ms=[round(x[0], 2) for x in reps])
         e2e_ms = reduce_max(e2e_ms, dist)
         e2e = {"value": whole_job_rate(world, vox_step, args.steps, e2e_ms), "unit": UNIT,
                "h2d_bytes_per_step": int((phase.nbytes + E.nbytes) / args.steps),
@@ -382,7 +391,7 @@ def run_gpu(args, rank, world, dist):
                                          + 6 * 8),
                "what": "operators from a host phase map, basic_scheme() for K iterations "
                        "(residuals read back every iteration), strain field copied to "
-                       "pinned host memory", "parts": parts}
+                       "pinned host memory; median of 3 repetitions", "parts": parts}
 
     solve = None
     if not args.no_solve and rank == 0 and world == 1:
@@ -800,7 +809,7 @@ def run_kernels(args, rank):
     from janus_b200.fft.serial import create_real
     from janus_b200.gradients import _gradient
     from janus_b200.green import filtered, truncated, willot2015
-    from janus_b200.solvers import BasicScheme, MixedScheme
+    from janus_b200.solvers import GMRES, BasicScheme, MixedScheme
 
     torch.cuda.set_device(env_int("LOCAL_RANK", 0))
     calls = []
@@ -856,6 +865,9 @@ def run_kernels(args, rank):
                     MixedScheme(g, loc, nload=2, inner=2, method=method).run(
                         E, tol=1e-30, max_outer=2)
                     calls.append(tag + " mixed scheme " + method)
+                # two cycles of GMRES(3): Arnoldi steps, restart, update
+                GMRES(g, loc, nload=2, restart=3).run(E, tol=1e-30, max_iter=5)
+                calls.append(tag + " gmres")
 
                 class _Cell:
                     pass

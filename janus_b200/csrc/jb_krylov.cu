@@ -268,31 +268,44 @@ __global__ void __launch_bounds__(kKrThreads)
 // ---------------------------------------------------------------------------
 constexpr int kGmChunk = 8;
 
-// partials[(l * kGmChunk + i) * nb + b] = block b's share of w . V_{j0+i}
+// partials[(l * kGmChunk + i) * nb + b] = block b's share of w . V_{j0+i},
+// i < CNT; VEC: two consecutive elements per access (every field 16-byte
+// aligned and nel even)
+template <int CNT, bool VEC>
 __global__ void __launch_bounds__(kKrThreads)
     gm_dots_kernel(int64_t nel, const double* __restrict__ w, const double* __restrict__ V,
-                   int64_t vs, int j0, int cnt, double* partials) {
+                   int64_t vs, int j0, double* partials) {
   __shared__ double red[kKrThreads / 32];
   const int l = blockIdx.y, nb = gridDim.x;
   const int64_t off = (int64_t)l * nel;
   const double* wl = w + off;
   const double* vb = V + (int64_t)j0 * vs + off;
-  double acc[kGmChunk];
+  double acc[CNT];
 #pragma unroll
-  for (int i = 0; i < kGmChunk; ++i) acc[i] = 0.0;
+  for (int i = 0; i < CNT; ++i) acc[i] = 0.0;
   const int64_t stride = (int64_t)nb * blockDim.x;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride) {
-    const double x = wl[e];
+  const int64_t e0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if constexpr (VEC) {
+    const double2* w2 = reinterpret_cast<const double2*>(wl);
+    for (int64_t e = e0; e < nel / 2; e += stride) {
+      const double2 x = w2[e];
 #pragma unroll
-    for (int i = 0; i < kGmChunk; ++i)
-      if (i < cnt) acc[i] += x * vb[(int64_t)i * vs + e];
+      for (int i = 0; i < CNT; ++i) {
+        const double2 v = reinterpret_cast<const double2*>(vb + (int64_t)i * vs)[e];
+        acc[i] += x.x * v.x + x.y * v.y;
+      }
+    }
+  } else {
+    for (int64_t e = e0; e < nel; e += stride) {
+      const double x = wl[e];
+#pragma unroll
+      for (int i = 0; i < CNT; ++i) acc[i] += x * vb[(int64_t)i * vs + e];
+    }
   }
 #pragma unroll
-  for (int i = 0; i < kGmChunk; ++i) {
-    if (i < cnt) {  // cnt is uniform over the block
-      const double t = kr_block_sum(acc[i], red);
-      if (threadIdx.x == 0) partials[((int64_t)l * kGmChunk + i) * nb + blockIdx.x] = t;
-    }
+  for (int i = 0; i < CNT; ++i) {
+    const double t = kr_block_sum(acc[i], red);
+    if (threadIdx.x == 0) partials[((int64_t)l * kGmChunk + i) * nb + blockIdx.x] = t;
   }
 }
 
@@ -308,29 +321,45 @@ __global__ void __launch_bounds__(kKrThreads)
   if (threadIdx.x == 0) out[(int64_t)l * ldo + o0 + i] = t;
 }
 
-// w += sign * sum_{i < cnt} coef[l * ldc + c0 + i] V_{j0+i}; with partials,
+// w += sign * sum_{i < CNT} coef[l * ldc + c0 + i] V_{j0+i}; with partials,
 // also block b's share of |w|^2 after the update at partials[l * kGmChunk * nb + b]
+template <int CNT, bool VEC>
 __global__ void __launch_bounds__(kKrThreads)
     gm_axpys_kernel(int64_t nel, double* __restrict__ w, const double* __restrict__ V,
-                    int64_t vs, int j0, int cnt, const double* __restrict__ coef, int ldc,
-                    int c0, double sign, double* partials) {
+                    int64_t vs, int j0, const double* __restrict__ coef, int ldc, int c0,
+                    double sign, double* partials) {
   __shared__ double red[kKrThreads / 32];
   const int l = blockIdx.y;
   const int64_t off = (int64_t)l * nel;
   double* wl = w + off;
   const double* vb = V + (int64_t)j0 * vs + off;
-  double a[kGmChunk];
+  double a[CNT];
 #pragma unroll
-  for (int i = 0; i < kGmChunk; ++i) a[i] = i < cnt ? sign * coef[(int64_t)l * ldc + c0 + i] : 0.0;
+  for (int i = 0; i < CNT; ++i) a[i] = sign * coef[(int64_t)l * ldc + c0 + i];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t e0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double nn = 0.0;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride) {
-    double x = wl[e];
+  if constexpr (VEC) {
+    double2* w2 = reinterpret_cast<double2*>(wl);
+    for (int64_t e = e0; e < nel / 2; e += stride) {
+      double2 x = w2[e];
 #pragma unroll
-    for (int i = 0; i < kGmChunk; ++i)
-      if (i < cnt) x += a[i] * vb[(int64_t)i * vs + e];
-    wl[e] = x;
-    nn += x * x;
+      for (int i = 0; i < CNT; ++i) {
+        const double2 v = reinterpret_cast<const double2*>(vb + (int64_t)i * vs)[e];
+        x.x += a[i] * v.x;
+        x.y += a[i] * v.y;
+      }
+      w2[e] = x;
+      nn += x.x * x.x + x.y * x.y;
+    }
+  } else {
+    for (int64_t e = e0; e < nel; e += stride) {
+      double x = wl[e];
+#pragma unroll
+      for (int i = 0; i < CNT; ++i) x += a[i] * vb[(int64_t)i * vs + e];
+      wl[e] = x;
+      nn += x * x;
+    }
   }
   if (partials) {  // uniform over the grid
     nn = kr_block_sum(nn, red);
@@ -347,23 +376,43 @@ __global__ void __launch_bounds__(kKrThreads)
   const double f = (n > 0.0 && isfinite(1.0 / n)) ? 1.0 / n : 0.0;
   double* wl = w + (int64_t)l * nel;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += stride)
-    wl[e] *= f;
+  const int64_t e0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t done = 0;
+  if (kr_vec4(nel, wl, wl, wl)) {  // 32-byte accesses
+    double4* w4 = reinterpret_cast<double4*>(wl);
+    for (int64_t e = e0; e < nel / 4; e += stride) {
+      double4 x = w4[e];
+      x.x *= f;
+      x.y *= f;
+      x.z *= f;
+      x.w *= f;
+      w4[e] = x;
+    }
+    done = nel / 4 * 4;
+  }
+  for (int64_t e = done + e0; e < nel; e += stride) wl[e] *= f;
 }
 
-// r = E_l - ax (the residual of the macroscopic load; r may alias ax)
+// r = E_l - ax (the residual of the macroscopic load; r may alias ax),
+// element-wise over the load case's nvox * C values: consecutive threads
+// take consecutive elements (component = element mod C)
 template <int C>
 __global__ void __launch_bounds__(kKrThreads)
     gm_resid_kernel(int64_t nvox, const double* __restrict__ E, const double* ax, double* r) {
   const int l = blockIdx.y;
-  const int64_t off = (int64_t)l * nvox * C;
+  const int64_t nel = nvox * C, off = (int64_t)l * nel;
   double e[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) e[c] = E[l * C + c];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += stride)
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nel; i += stride) {
+    const int c = (int)(i % C);
+    double ev = e[0];
 #pragma unroll
-    for (int c = 0; c < C; ++c) r[off + v * C + c] = e[c] - ax[off + v * C + c];
+    for (int q = 1; q < C; ++q)
+      if (c == q) ev = e[q];
+    r[off + i] = ev - ax[off + i];
+  }
 }
 
 int kr_blocks(int64_t nel, int L) {
@@ -380,13 +429,55 @@ int krylov_blocks(int64_t nel, int L) { return kr_blocks(nel, L); }
 
 int gmres_chunk() { return kGmChunk; }
 
+namespace {
+
+// every field of the call starts on a 16-byte boundary and holds an even
+// number of elements
+bool gm_vec2(int64_t nel, int64_t vs, const void* a, const void* b) {
+  return nel % 2 == 0 && vs % 2 == 0 &&
+         ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
+}
+
+template <int CNT>
+void gm_dots_go(bool vec, dim3 grid, cudaStream_t st, int64_t nel, const double* w,
+                const double* V, int64_t vs, int j0, double* partials) {
+  if (vec)
+    gm_dots_kernel<CNT, true><<<grid, kKrThreads, 0, st>>>(nel, w, V, vs, j0, partials);
+  else
+    gm_dots_kernel<CNT, false><<<grid, kKrThreads, 0, st>>>(nel, w, V, vs, j0, partials);
+}
+
+template <int CNT>
+void gm_axpys_go(bool vec, dim3 grid, cudaStream_t st, int64_t nel, double* w, const double* V,
+                 int64_t vs, int j0, const double* coef, int ldc, int c0, double sign,
+                 double* partials) {
+  if (vec)
+    gm_axpys_kernel<CNT, true><<<grid, kKrThreads, 0, st>>>(nel, w, V, vs, j0, coef, ldc, c0,
+                                                            sign, partials);
+  else
+    gm_axpys_kernel<CNT, false><<<grid, kKrThreads, 0, st>>>(nel, w, V, vs, j0, coef, ldc, c0,
+                                                             sign, partials);
+}
+
+}  // namespace
+
 cudaError_t launch_gmres_dots(int64_t nel, int L, const double* w, const double* V, int64_t vs,
                               int j0, int cnt, double* partials, double* out, int ldo, int o0,
                               cudaStream_t st) {
   if (cnt < 1 || cnt > kGmChunk) return cudaErrorInvalidValue;
   const int nb = kr_blocks(nel, L);
-  gm_dots_kernel<<<dim3((unsigned)nb, (unsigned)L), kKrThreads, 0, st>>>(nel, w, V, vs, j0, cnt,
-                                                                          partials);
+  const dim3 grid((unsigned)nb, (unsigned)L);
+  const bool vec = gm_vec2(nel, vs, w, V + (int64_t)j0 * vs);
+  switch (cnt) {
+    case 1: gm_dots_go<1>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    case 2: gm_dots_go<2>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    case 3: gm_dots_go<3>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    case 4: gm_dots_go<4>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    case 5: gm_dots_go<5>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    case 6: gm_dots_go<6>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    case 7: gm_dots_go<7>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+    default: gm_dots_go<8>(vec, grid, st, nel, w, V, vs, j0, partials); break;
+  }
   gm_reduce_kernel<<<dim3((unsigned)cnt, (unsigned)L), kKrThreads, 0, st>>>(partials, nb, out,
                                                                              ldo, o0);
   return cudaGetLastError();
@@ -398,8 +489,18 @@ cudaError_t launch_gmres_axpys(int64_t nel, int L, double* w, const double* V, i
   if (cnt < 1 || cnt > kGmChunk) return cudaErrorInvalidValue;
   if ((partials == nullptr) != (sq == nullptr)) return cudaErrorInvalidValue;
   const int nb = kr_blocks(nel, L);
-  gm_axpys_kernel<<<dim3((unsigned)nb, (unsigned)L), kKrThreads, 0, st>>>(
-      nel, w, V, vs, j0, cnt, coef, ldc, c0, sign, partials);
+  const dim3 grid((unsigned)nb, (unsigned)L);
+  const bool vec = gm_vec2(nel, vs, w, V + (int64_t)j0 * vs);
+  switch (cnt) {
+    case 1: gm_axpys_go<1>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    case 2: gm_axpys_go<2>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    case 3: gm_axpys_go<3>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    case 4: gm_axpys_go<4>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    case 5: gm_axpys_go<5>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    case 6: gm_axpys_go<6>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    case 7: gm_axpys_go<7>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+    default: gm_axpys_go<8>(vec, grid, st, nel, w, V, vs, j0, coef, ldc, c0, sign, partials); break;
+  }
   if (sq)
     gm_reduce_kernel<<<dim3(1u, (unsigned)L), kKrThreads, 0, st>>>(partials, nb, sq, 1, 0);
   return cudaGetLastError();
