@@ -25,7 +25,11 @@ from .solvers import MixedResult, MixedScheme
 
 class BatchedMixedScheme:
     """problems: sequence of (green_op, local_op, nload) triples (FP64
-    operators of janus_b200.green / operators, any grid size each)."""
+    operators of janus_b200.green / operators, any grid size each).
+
+    With method "bicgstab" every captured correction runs the full ``inner``
+    BiCGSTAB iterations (a lone MixedScheme sizes them adaptively); the
+    results equal one-by-one solves with method "bicgstab_fixed" bitwise."""
 
     def __init__(self, problems, inner=20, branches=8, method="basic"):
         if not problems:

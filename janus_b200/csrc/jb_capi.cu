@@ -377,9 +377,12 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
   }
   const AxisData& last = g->ax[dim - 1];
   if ((int64_t)L > 65535) return fail(JB_EINVAL, "batch too large (max 65535)");
+  // 2D spectral rows padded to 16 bytes (FP32, odd m * C); 3D rows (C = 6)
+  // always are
+  const int64_t sp = dim == 2 ? jb::spectral_pitch(g->dtype, m, C) : m * C;
   rec->mark(st);
-  JB_TRY(launch_status(jb::launch_rows_r2c(g->dtype, last, C, (int)L, x, geom, spec, local, st),
-                       "rows_r2c"));
+  JB_TRY(launch_status(
+      jb::launch_rows_r2c(g->dtype, last, C, (int)L, x, geom, spec, local, st, sp), "rows_r2c"));
   rec->mark(st);
   if (dim == 3) {
     JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[1], 0, L * n0, m * C, spec, spec, C,
@@ -400,7 +403,8 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
     gt.mn = nullptr;
   }
   JB_TRY(launch_status(jb::launch_cols(g->dtype, g->ax[0], 2, L, inner0, spec, spec, C, dim,
-                                       &gt, n1, m, st, &g->tune_green),
+                                       &gt, n1, m, st, &g->tune_green,
+                                       dim == 2 ? sp : inner0),
                        "cols_green_axis0"));
   rec->mark(st);
   if (dim == 3) {
@@ -420,17 +424,20 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
     scale = -scale;
   }
   JB_TRY(launch_status(jb::launch_rows_c2r(g->dtype, last, C, (int)L, spec, y, geom, scale, upd,
-                                           nb_rows, st),
+                                           nb_rows, st, sp),
                        "rows_c2r"));
   rec->mark(st);
   return JB_OK;
 }
 
+// complex elements of one field's internal half spectrum (2D rows padded as
+// green_passes lays them out)
 int64_t spec_elems(const jb_green* g) {
   const int C = g->dim == 2 ? 3 : 6;
   const int64_t nlast = g->dim == 2 ? g->n[1] : g->n[2];
   const int64_t m = nlast / 2 + 1;
-  return (g->dim == 2 ? g->n[0] : g->n[0] * g->n[1]) * m * C;
+  if (g->dim == 2) return g->n[0] * jb::spectral_pitch(g->dtype, m, C);
+  return g->n[0] * g->n[1] * m * C;
 }
 
 }  // namespace

@@ -148,6 +148,7 @@ template <typename T> struct RowsArgs {
   AxisPlan plan;
   RealGeom g;
   int R, W, m;
+  int64_t sp;  // spectral row pitch in complex elements (m * C, or one more)
   int L;       // load cases (persistent kernels)
   int contig;  // real side rows are contiguous [rows][n][C]
   int64_t cstride_l;
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
-  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
+  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + R);  // + R: a padded spectral row each
   T* Ar = reinterpret_cast<T*>(A);
   T* Br = reinterpret_cast<T*>(B);
   const int ldr = 2 * W;
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
   // local operator: phase ids of the tile and the (tr, dev) table go to
   // shared memory while the bulk copy is in flight
-  int* phs = reinterpret_cast<int*>(B + (size_t)(n + 2) * W);
+  int* phs = reinterpret_cast<int*>(B + (size_t)(n + 2) * W + R);
   T* tabs = align16_ptr<T>(phs + (size_t)R * n);
   const T* tab = a.table;
   if constexpr (LOCAL) {
@@ -361,15 +362,15 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       const C P = Z[k * W + col];
       const C Q = cconj(Z[(k == 0 ? 0 : n - k) * W + col]);
       if (ra < RC && rra < rows_here)
-        S[((int64_t)rra * m + k) * kC + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
+        S[(int64_t)rra * a.sp + k * kC + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
       if (rb < RC && rrb < rows_here)
-        S[((int64_t)rrb * m + k) * kC + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
+        S[(int64_t)rrb * a.sp + k * kC + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
     }
   }
   fence_async_shared();
   __syncthreads();
-  C* dst = a.out + l * a.cstride_l + row0 * m * kC;
-  const uint32_t obytes = (uint32_t)(rows_here * m * kC * sizeof(C));
+  C* dst = a.out + l * a.cstride_l + row0 * a.sp;
+  const uint32_t obytes = (uint32_t)(rows_here * a.sp * sizeof(C));
   if (aligned16(dst) && obytes % 16 == 0) {
     if (threadIdx.x == 0) {
       bulk_store(dst, S, obytes);
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       bulk_wait_read();
     }
   } else {
-    const int cnt = rows_here * m * kC;
+    const int cnt = (int)(rows_here * a.sp);
     for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) dst[idx] = S[idx];
   }
 }
@@ -409,15 +410,15 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
-  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W);
-  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W);  // [R][n][CC] side-field staging
+  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + R);  // + R: a padded spectral row each
+  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W + R);  // [R][n][CC] side-field staging
   const int ldr = 2 * W;
   const int l = blockIdx.y;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
   const int RC = R * kC;
-  const C* src = a.cin + l * a.cstride_l + row0 * m * kC;
-  const uint32_t sbytes = (uint32_t)(rows_here * m * kC * sizeof(C));
+  const C* src = a.cin + l * a.cstride_l + row0 * a.sp;
+  const uint32_t sbytes = (uint32_t)(rows_here * a.sp * sizeof(C));
   // side field: old eps (update, resid) or the right-hand side (rhs)
   const T* sidel = (EPI == kEpiRhs ? a.rhs : a.y) + l * a.g.ls;
   const T* sidechunk = sidel + row0 * n * kC;
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
     }
   }
   if (!bulk_s) {
-    const int cnt = rows_here * m * kC;
+    const int cnt = (int)(rows_here * a.sp);
     for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) B[idx] = src[idx];
   }
   if (kSide && !bulk_e) {
@@ -480,8 +481,8 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       const bool mirror = 2 * k > n;
       const int kk = mirror ? n - k : k;
       C Av = mkc(T(0), T(0)), Bv = mkc(T(0), T(0));
-      if (va) Av = B[((int64_t)rra * m + kk) * kC + ca];
-      if (vb) Bv = B[((int64_t)rrb * m + kk) * kC + cb];
+      if (va) Av = B[(int64_t)rra * a.sp + kk * kC + ca];
+      if (vb) Bv = B[(int64_t)rrb * a.sp + kk * kC + cb];
       if (kk == 0 || 2 * kk == n) {
         Av.y = T(0);
         Bv.y = T(0);
@@ -588,7 +589,8 @@ template <typename T> struct ColsArgs {
   cx<T>* out;
   const cx<T>* tw;
   AxisPlan plan;
-  int64_t inner;
+  int64_t inner;  // columns transformed
+  int64_t pitch;  // complex elements between consecutive rows (>= inner)
   int64_t outer;
   int W, C;
   int64_t m_last;
@@ -614,10 +616,10 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
   const int64_t c0 = (int64_t)blockIdx.x * W;
   const int Wc = (int)min((int64_t)W, a.inner - c0);
   const int64_t o = blockIdx.y;
-  const C* src = a.in + o * n * a.inner + c0;
-  C* dst = a.out + o * n * a.inner + c0;
+  const C* src = a.in + o * n * a.pitch + c0;
+  C* dst = a.out + o * n * a.pitch + c0;
   const uint32_t rowbytes = (uint32_t)(Wc * sizeof(C));
-  const bool bulk = aligned16(src) && aligned16(dst) && ((a.inner * sizeof(C)) % 16 == 0) &&
+  const bool bulk = aligned16(src) && aligned16(dst) && ((a.pitch * sizeof(C)) % 16 == 0) &&
                     (rowbytes % 16 == 0) && ((W * sizeof(C)) % 16 == 0);
   if (threadIdx.x == 0) {
     fail_flag = 0;
@@ -630,7 +632,7 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
       if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, rowbytes * (uint32_t)n);
       __syncwarp();
       for (int e = threadIdx.x; e < n; e += 32)
-        bulk_load(A + (size_t)e * W, src + (int64_t)e * a.inner, rowbytes, &bar);
+        bulk_load(A + (size_t)e * W, src + (int64_t)e * a.pitch, rowbytes, &bar);
     }
     if (Wc < W)
       for (int idx = threadIdx.x; idx < n * (W - Wc); idx += blockDim.x) {
@@ -641,7 +643,7 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
     for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
       const int e = idx / W;
       const int col = idx - e * W;
-      A[idx] = col < Wc ? src[(int64_t)e * a.inner + col] : mkc(T(0), T(0));
+      A[idx] = col < Wc ? src[(int64_t)e * a.pitch + col] : mkc(T(0), T(0));
     }
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
@@ -690,7 +692,7 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
     __syncthreads();
     if (threadIdx.x < 32) {
       for (int e = threadIdx.x; e < n; e += 32)
-        bulk_store(dst + (int64_t)e * a.inner, Z + (size_t)e * W, rowbytes);
+        bulk_store(dst + (int64_t)e * a.pitch, Z + (size_t)e * W, rowbytes);
       bulk_commit();
       bulk_wait_read();
     }
@@ -698,7 +700,7 @@ __global__ void __launch_bounds__(kThreads) cols_kernel(ColsArgs<T> a) {
     for (int idx = threadIdx.x; idx < n * W; idx += blockDim.x) {
       const int e = idx / W;
       const int col = idx - e * W;
-      if (col < Wc) dst[(int64_t)e * a.inner + col] = Z[idx];
+      if (col < Wc) dst[(int64_t)e * a.pitch + col] = Z[idx];
     }
   }
 }
@@ -1122,8 +1124,10 @@ size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local,
   const size_t treal = (size_t)nphase * entry;
   const size_t staged = treal <= 2 * (size_t)kTabStage ? treal : 0;
   auto a16 = [](size_t v) { return (v + 15) / 16 * 16; };
-  size_t off = a16(n * cs) + (size_t)(n + 2) * w * cs;  // twiddles | A
-  off = a16(off) + (size_t)(n + 2) * w * cs;           // B
+  // twiddles | A | B; A and B hold (n + 2) w complex plus r for the padding
+  // of r spectral rows
+  size_t off = a16(n * cs) + ((size_t)(n + 2) * w + r) * cs;
+  off = a16(off) + ((size_t)(n + 2) * w + r) * cs;
   if (update) off = a16(off) + (size_t)r * n * C * (cs / 2) + (size_t)(r - 1) * 32;
   if (local) off = a16(off + (size_t)r * n * 4) + staged * (cs / 2);
   return off;
@@ -1266,13 +1270,13 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // 3D map of a complex [outer][n][inner] array seen as reals [outer][n][2 inner],
 // box = 2W reals x nbox rows x 1
-bool make_cols_map(CUtensorMap* m, const void* base, bool f64, int64_t inner, int n,
-                   int64_t outer, int W, int nbox) {
+bool make_cols_map(CUtensorMap* m, const void* base, bool f64, int64_t inner, int64_t pitch,
+                   int n, int64_t outer, int W, int nbox) {
   auto enc = tensor_map_encoder();
   if (!enc) return false;
   const cuuint64_t rs = f64 ? 8 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)(2 * inner), (cuuint64_t)n, (cuuint64_t)outer};
-  cuuint64_t strides[2] = {(cuuint64_t)(2 * inner) * rs, (cuuint64_t)(2 * inner) * rs * n};
+  cuuint64_t strides[2] = {(cuuint64_t)(2 * pitch) * rs, (cuuint64_t)(2 * pitch) * rs * n};
   cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)nbox, 1};
   cuuint32_t es[3] = {1, 1, 1};
   const CUresult r = enc(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
@@ -1356,7 +1360,7 @@ cudaError_t c2r_ct_dispatch(int C, int epi, const RowsArgs<T>& a, dim3 grid, siz
 
 template <typename T>
 cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const RealGeom& g,
-                       void* out, const LocalDesc* local, cudaStream_t st) {
+                       void* out, const LocalDesc* local, cudaStream_t st, int64_t spitch) {
   RowsArgs<T> a{};
   int R, W;
   size_t smem;
@@ -1376,8 +1380,10 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   a.R = R;
   a.W = W;
   a.m = n / 2 + 1;
+  a.sp = spitch > 0 ? spitch : (int64_t)a.m * C;
+  if (a.sp < (int64_t)a.m * C || a.sp > (int64_t)a.m * C + 1) return cudaErrorInvalidValue;
   a.contig = contiguous_rows(g, n, C);
-  a.cstride_l = g.rows * a.m * C;
+  a.cstride_l = g.rows * a.sp;
   a.L = L;
   if (local) {
     a.phase = local->phase;
@@ -1429,7 +1435,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
 template <typename T>
 cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y,
                        const RealGeom& g, double scale, const UpdateDesc* upd, int* nb_out,
-                       cudaStream_t st) {
+                       cudaStream_t st, int64_t spitch) {
   RowsArgs<T> a{};
   int R, W;
   size_t smem;
@@ -1446,8 +1452,10 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
   a.R = R;
   a.W = W;
   a.m = n / 2 + 1;
+  a.sp = spitch > 0 ? spitch : (int64_t)a.m * C;
+  if (a.sp < (int64_t)a.m * C || a.sp > (int64_t)a.m * C + 1) return cudaErrorInvalidValue;
   a.contig = contiguous_rows(g, n, C);
-  a.cstride_l = g.rows * a.m * C;
+  a.cstride_l = g.rows * a.sp;
   a.scale = static_cast<T>(scale);
   a.L = L;
   const int epi = upd ? upd->mode : kEpiPlain;
@@ -1566,7 +1574,7 @@ cudaError_t cols_tma_launch(const CUtensorMap& tin, const CUtensorMap& tout,
 template <typename T>
 cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, const void* in,
                    void* out, int C, int dim, const GreenDeviceTables* gt, int64_t m_last,
-                   cudaStream_t st, const ColsTuning* tune) {
+                   cudaStream_t st, const ColsTuning* tune, int64_t pitch) {
   ColsArgs<T> a{};
   int W;
   size_t smem;
@@ -1580,6 +1588,8 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
   a.tw = static_cast<const cx<T>*>(ax.tw);
   a.plan = ax.plan;
   a.inner = inner;
+  a.pitch = pitch > 0 ? pitch : inner;
+  if (a.pitch < inner) return cudaErrorInvalidValue;
   a.W = W;
   a.C = C;
   a.m_last = m_last;
@@ -1590,15 +1600,17 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     int Wp, nbuf;
     size_t sp;
     const size_t cs = sizeof(cx<T>);
-    if (al16(in) && al16(out) && (inner * cs) % 16 == 0 &&
+    // rows 16-byte aligned; a last chunk reaching past `inner` is zero-filled
+    // by the load and clipped by the store
+    if (al16(in) && al16(out) && (a.pitch * cs) % 16 == 0 &&
         cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &Wp, &sp, &nbuf,
                        mode == 2 && a.mn == nullptr, tune)) {
       int nbox = n <= 256 ? n : 256;  // rows per box: largest divisor of n up to 256
       while (n % nbox != 0) --nbox;
       CUtensorMap tin, tout;
       if (nbox >= 8 &&
-          make_cols_map(&tin, in, sizeof(T) == 8, inner, n, outer, Wp, nbox) &&
-          make_cols_map(&tout, out, sizeof(T) == 8, inner, n, outer, Wp, nbox)) {
+          make_cols_map(&tin, in, sizeof(T) == 8, inner, a.pitch, n, outer, Wp, nbox) &&
+          make_cols_map(&tout, out, sizeof(T) == 8, inner, a.pitch, n, outer, Wp, nbox)) {
         ColsArgs<T> b = a;
         b.W = Wp;
         b.nbuf = nbuf;
@@ -1641,26 +1653,26 @@ cudaError_t read_and_clear_fault(unsigned* out) {
 
 cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const void* x,
                             const RealGeom& g, void* out, const LocalDesc* local,
-                            cudaStream_t st) {
-  return dtype == F64 ? rows_r2c_t<double>(ax, C, L, x, g, out, local, st)
-                      : rows_r2c_t<float>(ax, C, L, x, g, out, local, st);
+                            cudaStream_t st, int64_t spitch) {
+  return dtype == F64 ? rows_r2c_t<double>(ax, C, L, x, g, out, local, st, spitch)
+                      : rows_r2c_t<float>(ax, C, L, x, g, out, local, st, spitch);
 }
 
 cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const void* in,
                             void* y, const RealGeom& g, double scale, const UpdateDesc* upd,
-                            int* nb_out, cudaStream_t st) {
-  return dtype == F64 ? rows_c2r_t<double>(ax, C, L, in, y, g, scale, upd, nb_out, st)
-                      : rows_c2r_t<float>(ax, C, L, in, y, g, scale, upd, nb_out, st);
+                            int* nb_out, cudaStream_t st, int64_t spitch) {
+  return dtype == F64 ? rows_c2r_t<double>(ax, C, L, in, y, g, scale, upd, nb_out, st, spitch)
+                      : rows_c2r_t<float>(ax, C, L, in, y, g, scale, upd, nb_out, st, spitch);
 }
 
 cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer, int64_t inner,
                         const void* in, void* out, int C, int dim,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
-                        cudaStream_t st, const ColsTuning* tune) {
+                        cudaStream_t st, const ColsTuning* tune, int64_t pitch) {
   (void)n1;
   return dtype == F64
-             ? cols_t<double>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st, tune)
-             : cols_t<float>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st, tune);
+             ? cols_t<double>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st, tune, pitch)
+             : cols_t<float>(ax, mode, outer, inner, in, out, C, dim, gt, m_last, st, tune, pitch);
 }
 
 cudaError_t launch_local(int dtype, const LocalDesc& loc, int C, int L, int64_t nvox,

@@ -107,15 +107,26 @@ int max_axis_length(int dtype);
 // bit 0: a kernel gave up a bounded wait (see jb_async.cuh); cleared on read
 cudaError_t read_and_clear_fault(unsigned* out);
 
-// r2c along the contiguous axis: real x (geom) -> complex out [L][rows][m][C].
+// Spectral row pitch (complex elements) of the solver's internal half
+// spectrum: m * C, plus one where FP32 rows of m * C complex would not span a
+// multiple of 16 bytes (2D, C = 3, m odd), so that rows start on 16-byte
+// boundaries and the column passes can use tensor TMA.
+inline int64_t spectral_pitch(int dtype, int64_t m, int C) {
+  const int64_t p = m * C;
+  return (dtype == F32 && (p % 2) != 0) ? p + 1 : p;
+}
+// r2c along the contiguous axis: real x (geom) -> complex out [L][rows][sp]
+// (the first m * C of each row's sp complex elements; sp = spitch, default
+// m * C, at most m * C + 1).
 cudaError_t launch_rows_r2c(int dtype, const AxisData& ax, int C, int L, const void* x,
                             const RealGeom& g, void* out, const LocalDesc* local,
-                            cudaStream_t st);
-// c2r along the contiguous axis: complex in [L][rows][m][C] -> real y (geom),
+                            cudaStream_t st, int64_t spitch = 0);
+// c2r along the contiguous axis: complex in [L][rows][sp] -> real y (geom),
 // y = scale * c2r(in), or the solver update when upd != nullptr.
 cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const void* in,
                             void* y, const RealGeom& g, double scale,
-                            const UpdateDesc* upd, int* nblocks_out, cudaStream_t st);
+                            const UpdateDesc* upd, int* nblocks_out, cudaStream_t st,
+                            int64_t spitch = 0);
 // tile schedule of a column pass (0 = the built-in rule): tile width in
 // complex columns (a multiple of the coefficient size for the Green pass),
 // rotating input tiles (2 or 3), and whether compile-time FFT tiles may be
@@ -126,13 +137,15 @@ struct ColsTuning {
   int ct = 1;
 };
 
-// complex transform along a strided axis of [outer][n][inner] (complex units).
+// complex transform along a strided axis of [outer][n][pitch] (complex
+// units; the first `inner` of each row's `pitch` elements, pitch 0 = inner).
 // mode 0: forward, 1: inverse, 2: forward -> Green contraction -> inverse
 // (axis 0 only; dim/m_last/grid describe the spectrum for the contraction).
 cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer,
                         int64_t inner, const void* in, void* out, int C, int dim,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
-                        cudaStream_t st, const ColsTuning* tune = nullptr);
+                        cudaStream_t st, const ColsTuning* tune = nullptr,
+                        int64_t pitch = 0);
 // M/N table of the Green operator on the half spectrum of an n0 x n1 (x n2)
 // grid: table[(f12 * n0 + b0) * NT + c], f12 = b1 * m + b2 (3D) or b1 (2D),
 // NT = 21 (3D) / 8 (2D).  `out` has n0 * n1 * m * NT (3D) reals of the dtype.
