@@ -407,7 +407,6 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int n = NCT > 0 ? NCT : a.plan.n;
   const int W = WCT > 0 ? WCT : a.W;
   const int R = WCT > 0 ? 2 * WCT / CC : a.R;
-  const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
   C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + R);  // + R: a padded spectral row each
