@@ -170,6 +170,48 @@ def test_invalid_shapes(variant):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["truncated", "filtered"])
+@pytest.mark.parametrize("shape", [(64, 64), (31, 45), (48, 62), (1, 8), (128, 96),
+                                   (256, 256), (9, 7, 5), (32, 24, 16)])
+def test_apply_random_fields_fp32_vs_oracle(variant, shape):
+    """FP32 apply, including 2D grids whose half-spectrum rows of m * 3
+    complex floats are padded to 16 bytes inside the solver passes (m odd:
+    64, 45, 96, 256; m even: 62), against the FP64 oracle."""
+    rng = np.random.default_rng(12)
+    s = 3 if len(shape) == 2 else 6
+    x = rng.normal(size=shape + (s,))
+    g = FACTORY[variant](material.create(MU, NU, len(shape)).green_operator(), shape, 0.5,
+                         dtype="float32")
+    y = g.apply(torch.from_numpy(x).float().cuda()).double().cpu().numpy()
+    ref = O.green_apply(x, MU, NU, 0.5, variant)
+    assert np.abs(y - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(64, 64), (45, 31), (96, 62)])
+def test_fp32_2d_basic_scheme_vs_oracle(shape):
+    """The FP32 2D solver passes (local operator in the first, update and
+    residual in the last, padded spectral rows between) against the oracle's
+    FP64 iterates."""
+    from janus_b200 import microstructures as micro
+    from janus_b200 import operators as ops
+    from janus_b200.solvers import BasicScheme
+    phase = (micro.ellipses(max(shape), 4, seed=2)[:shape[0], :shape[1]] > 0).astype(np.uint8)
+    pars = [O.delta_c(1.0, 0.3, 5.5, 0.3, 2), O.delta_c(10.0, 0.25, 5.5, 0.3, 2)]
+    tens = [ops.isotropic_4(a, b, 2) for a, b in pars]
+    loc = ops.BlockDiagonalOperator2D.from_phases(phase, tens, dtype=torch.float32)
+    g = truncated(material.create(5.5, 0.3, 2).green_operator(), shape, 1.0,
+                  dtype=torch.float32)
+    E = np.array([0.0, 0.0, 1.0])
+    r = BasicScheme(g, loc).run(E, 10)
+    eps_o, res_o, _ = O.basic_scheme(phase, [p[0] for p in pars], [p[1] for p in pars], 5.5,
+                                     0.3, E, 10)
+    eps = r.eps[0].double().cpu().numpy()
+    assert np.abs(eps - eps_o).max() <= 1e-5 * np.abs(eps_o).max()
+    np.testing.assert_allclose(r.residuals[:, 0], res_o, rtol=1e-3)
+
+
+@pytest.mark.gpu
 def test_batched_apply_and_fp32():
     rng = np.random.default_rng(8)
     shape = (32, 24, 16)
