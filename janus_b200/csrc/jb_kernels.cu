@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
-  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + R);  // + R: a padded spectral row each
+  // + R complex when spectral rows are padded (one element a row)
+  const int padr = a.sp > (int64_t)(n / 2 + 1) * CC ? R : 0;
+  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + padr);
   T* Ar = reinterpret_cast<T*>(A);
   T* Br = reinterpret_cast<T*>(B);
   const int ldr = 2 * W;
@@ -295,7 +297,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = a.tw[i];
   // local operator: phase ids of the tile and the (tr, dev) table go to
   // shared memory while the bulk copy is in flight
-  int* phs = reinterpret_cast<int*>(B + (size_t)(n + 2) * W + R);
+  int* phs = reinterpret_cast<int*>(B + (size_t)(n + 2) * W + padr);
   T* tabs = align16_ptr<T>(phs + (size_t)R * n);
   const T* tab = a.table;
   if constexpr (LOCAL) {
@@ -409,8 +411,10 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int R = WCT > 0 ? 2 * WCT / CC : a.R;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
-  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + R);  // + R: a padded spectral row each
-  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W + R);  // [R][n][CC] side-field staging
+  // + R complex when spectral rows are padded (one element a row)
+  const int padr = a.sp > (int64_t)(n / 2 + 1) * CC ? R : 0;
+  C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + padr);
+  T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W + padr);  // [R][n][CC] side-field staging
   const int ldr = 2 * W;
   const int l = blockIdx.y;
   const int64_t row0 = (int64_t)blockIdx.x * R;
@@ -1117,28 +1121,29 @@ int tile_threads(int W) {
 // the kernels' exact layout (each region aligned to 16 bytes): three CTAs
 // per SM of the FP64 c2r update kernel at n = 128 fit with 96 bytes to spare.
 size_t rows_smem(int dtype, int n, int C, int r, int w, bool update, bool local, int nphase,
-                 int entry = 2) {
+                 int entry = 2, bool padded = false) {
   const size_t cs = dtype == F64 ? 16 : 8;
   // staged table reals (2 * kTabStage at most)
   const size_t treal = (size_t)nphase * entry;
   const size_t staged = treal <= 2 * (size_t)kTabStage ? treal : 0;
   auto a16 = [](size_t v) { return (v + 15) / 16 * 16; };
-  // twiddles | A | B; A and B hold (n + 2) w complex plus r for the padding
-  // of r spectral rows
-  size_t off = a16(n * cs) + ((size_t)(n + 2) * w + r) * cs;
-  off = a16(off) + ((size_t)(n + 2) * w + r) * cs;
+  // twiddles | A | B; A and B hold (n + 2) w complex, plus r for the padding
+  // of r spectral rows when the rows are padded
+  const size_t pr = padded ? (size_t)r : 0;
+  size_t off = a16(n * cs) + ((size_t)(n + 2) * w + pr) * cs;
+  off = a16(off) + ((size_t)(n + 2) * w + pr) * cs;
   if (update) off = a16(off) + (size_t)r * n * C * (cs / 2) + (size_t)(r - 1) * 32;
   if (local) off = a16(off + (size_t)r * n * 4) + staged * (cs / 2);
   return off;
 }
 
 bool rows_shape(int dtype, int n, int C, bool update, int* R, int* W, size_t* smem,
-                bool local = false, int nphase = 0, int entry = 2) {
+                bool local = false, int nphase = 0, int entry = 2, bool padded = false) {
   const size_t cs = dtype == F64 ? 16 : 8;
   int r = (24 + C - 1) / C;
   for (;;) {
     const int w = (r * C + 1) / 2;
-    const size_t bytes = rows_smem(dtype, n, C, r, w, update, local, nphase, entry);
+    const size_t bytes = rows_smem(dtype, n, C, r, w, update, local, nphase, entry, padded);
     if (bytes <= kSmemBudget || r == 1) {
       if (bytes > kSmemCap - 4096) return false;
       *R = r;
@@ -1368,8 +1373,9 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   if (local && C == 1) return cudaErrorInvalidValue;
   const int nphase = local ? local->nphase : 0;
   const int entry = local ? local_entry(local->kind, local->dim) : 2;
+  const bool padded = spitch > (int64_t)(n / 2 + 1) * C;
   if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, false, &R, &W, &smem, local != nullptr,
-                  nphase, entry))
+                  nphase, entry, padded))
     return cudaErrorInvalidValue;
   a.x = static_cast<const T*>(x);
   a.out = static_cast<cx<T>*>(out);
@@ -1397,7 +1403,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     const int wct = n <= 128 ? 12 : 6;
     const int rct = 2 * wct / C;
     const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, false,
-                                 local != nullptr, nphase, entry);
+                                 local != nullptr, nphase, entry, padded);
     if (sct <= kSmemBudget + 24 * 1024) {
       RowsArgs<T> b = a;
       b.R = rct;
@@ -1441,7 +1447,9 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
   const int n = ax.plan.n;
   if (C != 1 && C != 3 && C != 6) return cudaErrorInvalidValue;
   if (upd && C == 1) return cudaErrorInvalidValue;
-  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, upd != nullptr, &R, &W, &smem))
+  const bool padded = spitch > (int64_t)(n / 2 + 1) * C;
+  if (!rows_shape(sizeof(T) == 8 ? F64 : F32, n, C, upd != nullptr, &R, &W, &smem, false, 0, 2,
+                  padded))
     return cudaErrorInvalidValue;
   a.cin = static_cast<const cx<T>*>(in);
   a.y = static_cast<T*>(upd ? upd->eps : y);
@@ -1471,7 +1479,7 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
     const int wct = n <= 128 ? 12 : 6;
     const int rct = 2 * wct / C;
     const size_t sct = rows_smem(sizeof(T) == 8 ? F64 : F32, n, C, rct, wct, upd != nullptr,
-                                 false, 0);
+                                 false, 0, 2, padded);
     if (sct <= kSmemBudget + 24 * 1024) {
       RowsArgs<T> b = a;
       b.R = rct;
