@@ -253,8 +253,11 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int m = n / 2 + 1;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
-  // + R complex when spectral rows are padded (one element a row)
-  const int padr = a.sp > (int64_t)(n / 2 + 1) * CC ? R : 0;
+  // spectral row pitch: six-component rows are never padded (m * 6 complex
+  // is even), so theirs is a compile-time constant; + R complex in the
+  // staging buffers when rows are padded (one element a row)
+  const int64_t sp = CC == 6 ? (int64_t)(n / 2 + 1) * 6 : a.sp;
+  const int padr = (CC != 6 && sp > (int64_t)(n / 2 + 1) * CC) ? R : 0;
   C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + padr);
   T* Ar = reinterpret_cast<T*>(A);
   T* Br = reinterpret_cast<T*>(B);
@@ -364,15 +367,15 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       const C P = Z[k * W + col];
       const C Q = cconj(Z[(k == 0 ? 0 : n - k) * W + col]);
       if (ra < RC && rra < rows_here)
-        S[(int64_t)rra * a.sp + k * kC + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
+        S[(int64_t)rra * sp + k * kC + ca] = mkc(T(0.5) * (P.x + Q.x), T(0.5) * (P.y + Q.y));
       if (rb < RC && rrb < rows_here)
-        S[(int64_t)rrb * a.sp + k * kC + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
+        S[(int64_t)rrb * sp + k * kC + cb] = mkc(T(0.5) * (P.y - Q.y), T(-0.5) * (P.x - Q.x));
     }
   }
   fence_async_shared();
   __syncthreads();
-  C* dst = a.out + l * a.cstride_l + row0 * a.sp;
-  const uint32_t obytes = (uint32_t)(rows_here * a.sp * sizeof(C));
+  C* dst = a.out + l * a.cstride_l + row0 * sp;
+  const uint32_t obytes = (uint32_t)(rows_here * sp * sizeof(C));
   if (aligned16(dst) && obytes % 16 == 0) {
     if (threadIdx.x == 0) {
       bulk_store(dst, S, obytes);
@@ -380,7 +383,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       bulk_wait_read();
     }
   } else {
-    const int cnt = (int)(rows_here * a.sp);
+    const int cnt = (int)(rows_here * sp);
     for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) dst[idx] = S[idx];
   }
 }
@@ -411,8 +414,9 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int R = WCT > 0 ? 2 * WCT / CC : a.R;
   C* tw = reinterpret_cast<C*>(smem);
   C* A = align16_ptr<C>(tw + n);
-  // + R complex when spectral rows are padded (one element a row)
-  const int padr = a.sp > (int64_t)(n / 2 + 1) * CC ? R : 0;
+  // spectral row pitch (compile-time for six components, see rows_r2c)
+  const int64_t sp = CC == 6 ? (int64_t)(n / 2 + 1) * 6 : a.sp;
+  const int padr = (CC != 6 && sp > (int64_t)(n / 2 + 1) * CC) ? R : 0;
   C* B = align16_ptr<C>(A + (size_t)(n + 2) * W + padr);
   T* Eo = align16_ptr<T>(B + (size_t)(n + 2) * W + padr);  // [R][n][CC] side-field staging
   const int ldr = 2 * W;
@@ -420,8 +424,8 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int rows_here = (int)min((int64_t)R, a.g.rows - row0);
   const int RC = R * kC;
-  const C* src = a.cin + l * a.cstride_l + row0 * a.sp;
-  const uint32_t sbytes = (uint32_t)(rows_here * a.sp * sizeof(C));
+  const C* src = a.cin + l * a.cstride_l + row0 * sp;
+  const uint32_t sbytes = (uint32_t)(rows_here * sp * sizeof(C));
   // side field: old eps (update, resid) or the right-hand side (rhs)
   const T* sidel = (EPI == kEpiRhs ? a.rhs : a.y) + l * a.g.ls;
   const T* sidechunk = sidel + row0 * n * kC;
@@ -457,7 +461,7 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
     }
   }
   if (!bulk_s) {
-    const int cnt = (int)(rows_here * a.sp);
+    const int cnt = (int)(rows_here * sp);
     for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) B[idx] = src[idx];
   }
   if (kSide && !bulk_e) {
@@ -484,8 +488,8 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), rows_min_blocks<
       const bool mirror = 2 * k > n;
       const int kk = mirror ? n - k : k;
       C Av = mkc(T(0), T(0)), Bv = mkc(T(0), T(0));
-      if (va) Av = B[(int64_t)rra * a.sp + kk * kC + ca];
-      if (vb) Bv = B[(int64_t)rrb * a.sp + kk * kC + cb];
+      if (va) Av = B[(int64_t)rra * sp + kk * kC + ca];
+      if (vb) Bv = B[(int64_t)rrb * sp + kk * kC + cb];
       if (kk == 0 || 2 * kk == n) {
         Av.y = T(0);
         Bv.y = T(0);
@@ -1386,7 +1390,9 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
   a.W = W;
   a.m = n / 2 + 1;
   a.sp = spitch > 0 ? spitch : (int64_t)a.m * C;
-  if (a.sp < (int64_t)a.m * C || a.sp > (int64_t)a.m * C + 1) return cudaErrorInvalidValue;
+  if (a.sp < (int64_t)a.m * C || a.sp > (int64_t)a.m * C + 1 ||
+      (C == 6 && a.sp != (int64_t)a.m * C))
+    return cudaErrorInvalidValue;
   a.contig = contiguous_rows(g, n, C);
   a.cstride_l = g.rows * a.sp;
   a.L = L;
@@ -1460,7 +1466,9 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
   a.W = W;
   a.m = n / 2 + 1;
   a.sp = spitch > 0 ? spitch : (int64_t)a.m * C;
-  if (a.sp < (int64_t)a.m * C || a.sp > (int64_t)a.m * C + 1) return cudaErrorInvalidValue;
+  if (a.sp < (int64_t)a.m * C || a.sp > (int64_t)a.m * C + 1 ||
+      (C == 6 && a.sp != (int64_t)a.m * C))
+    return cudaErrorInvalidValue;
   a.contig = contiguous_rows(g, n, C);
   a.cstride_l = g.rows * a.sp;
   a.scale = static_cast<T>(scale);
