@@ -1,7 +1,8 @@
 // Asynchronous bulk copies between global and shared memory (the TMA engine's
 // non-tensor form, cp.async.bulk) completed on an mbarrier, for sm_100a.
 //
-// No cluster multicast is used anywhere.  Every wait is bounded: after
+// Every copy lands in the issuing CTA's own shared memory (no copy is shared
+// across the CTAs of a cluster).  Every wait is bounded: after
 // kWaitLimit polls the kernel records a timeout in g_jb_fault (read by
 // jb_device_status on the host), waits once more (bounded) for its own
 // copies, and the caller returns without touching the tile.
@@ -104,9 +105,9 @@ __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// tiled tensor copies (TMA) through a CUtensorMap kernel parameter; no
-// multicast.  The box's innermost coordinate x times the element size is a
-// multiple of 16 bytes at every call site.
+// tiled tensor copies (TMA) through a CUtensorMap kernel parameter, into or
+// out of this CTA's shared memory only.  The box's innermost coordinate x
+// times the element size is a multiple of 16 bytes at every call site.
 __device__ __forceinline__ void tma_load_3d(void* sdst, const CUtensorMap* map, int x, int y,
                                             int z, uint64_t* bar) {
   asm volatile(
