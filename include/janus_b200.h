@@ -135,7 +135,9 @@ int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
  * reference plans with FFTW).  v[6] = {plain width, plain input tiles, plain
  * compile-time tiles allowed, Green width, Green input tiles, Green
  * compile-time tiles allowed}; widths in complex columns (the Green one a
- * multiple of s), input tiles 2 or 3, 0 = built-in rule.  A width whose
+ * multiple of s), input tiles 2 or 3, 0 = built-in rule; a Green
+ * compile-time value of 2 transforms the Green tiles in place (24 columns at
+ * n = 128, 12 at n = 256, no partner tile).  A width whose
  * tiles do not fit the shared-memory budget is narrowed.  An optional 7th
  * value selects the Green contraction: 0 built-in rule (the M/N table for
  * the filtered operator, on the fly for the truncated and finite-difference

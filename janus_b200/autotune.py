@@ -6,7 +6,8 @@ FFT radices follow from the axis length (compile-time radix-16/8 tiles for
 n = 64, 128, 256; runtime mixed-radix plans otherwise); what is tuned is how
 the column passes tile the spectrum: the width of a tile in complex columns,
 how many input tiles rotate through shared memory, whether the compile-time
-tiles are used, and whether the Green contraction reads the per-coefficient
+tiles are used (for the Green pass also in place, without a partner tile,
+24 columns wide at n = 128 and 12 at n = 256), and whether the Green contraction reads the per-coefficient
 M/N table or evaluates the operator on the fly.  Each candidate is timed on the solver step it
 will serve (CUDA events around every pass, several steps after a warm-up),
 the plain passes (3D axis 1) and the Green pass independently, and the
@@ -52,6 +53,9 @@ def candidates(dim, dtype):
     plain = [(w, nb, 1) for w in (4, 8, 16) for nb in (2, 3)] + [(8, 2, 0), (8, 3, 0)]
     green = [(w, nb, 1) for w in (s, 2 * s, 3 * s) for nb in (2, 3)] + [(s, 2, 0),
                                                                           (2 * s, 2, 0)]
+    # tiles transformed in place: 24 columns at n = 128, 12 at n = 256 (other
+    # lengths run these as ordinary compile-time or runtime-plan tiles)
+    green += [(24, 2, 2), (12, 2, 2)]
     return (plain if dim == 3 else []), green
 
 

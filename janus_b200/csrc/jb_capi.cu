@@ -710,12 +710,14 @@ int jb_green_set_tuning(jb_green* G, const int* v, int count) {
     return fail(JB_EINVAL, "tile widths must be in [0, 128], the Green one a multiple of s");
   for (int k : {v[1], v[4]})
     if (k != 0 && k != 2 && k != 3) return fail(JB_EINVAL, "input tiles must be 0, 2 or 3");
+  if (v[5] < 0 || v[5] > 2)
+    return fail(JB_EINVAL, "Green compile-time value must be 0, 1 or 2 (in place)");
   G->tune_plain.w = v[0];
   G->tune_plain.nbuf = v[1];
   G->tune_plain.ct = v[2] != 0;
   G->tune_green.w = v[3];
   G->tune_green.nbuf = v[4];
-  G->tune_green.ct = v[5] != 0;
+  G->tune_green.ct = v[5];
   if (count == 7) G->tune_table = v[6];
   return JB_OK;
 }

@@ -742,10 +742,9 @@ template <typename T, int MODE, int NCT> constexpr int cols_min_blocks() {
   return (MODE == 2 && NCT > 0) ? (sizeof(T) == 8 ? 2 : 4) : 1;
 }
 
-template <typename T, int MODE, int DIM, int NCT = 0, int WCT = 0>
-__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<T, MODE, NCT>())
-    cols_tma_kernel(const __grid_constant__ CUtensorMap tin,
-                    const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
+template <typename T, int MODE, int DIM, int NCT, int WCT, bool INPL>
+__device__ __forceinline__ void cols_tma_body(const CUtensorMap& tin, const CUtensorMap& tout,
+                                              const ColsArgs<T>& a, int nbox) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[3];
@@ -762,8 +761,9 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<
   auto in_tile = [&](int b) {
     return reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(In0) + b * tstride);
   };
-  C* Wk = in_tile(nbuf);
-  AxisK<T>* ax0 = align128_ptr<AxisK<T>>(Wk + tile);  // MODE 2: axis-0 Green values
+  // ping-pong partner of the transforms (none when they run in place)
+  C* Wk = INPL ? nullptr : in_tile(nbuf);
+  AxisK<T>* ax0 = align128_ptr<AxisK<T>>(INPL ? in_tile(nbuf) : Wk + tile);  // MODE 2: axis-0 values
   const int64_t ntx = (a.inner + W - 1) / W;
   const int64_t total = ntx * a.outer;
   if (threadIdx.x == 0) {
@@ -832,7 +832,13 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<
       for (int q = threadIdx.x; q < lines; q += blockDim.x) prefetch_l1(base + (size_t)q * 128);
     }
     C* Z;
-    if constexpr (NCT > 0) {
+    if constexpr (INPL) {
+      if (MODE == 1)
+        fft_ct_inplace<NCT, WCT, +1>(in, tw);
+      else
+        fft_ct_inplace<NCT, WCT, -1>(in, tw);
+      Z = in;
+    } else if constexpr (NCT > 0) {
       if (MODE == 1)
         Z = fft_ct<NCT, WCT, +1>(in, Wk, tw);
       else
@@ -882,14 +888,16 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<
       }
       __syncthreads();
       C* other = (Z == in) ? Wk : in;
-      if constexpr (NCT > 0)
+      if constexpr (INPL)
+        fft_ct_inplace<NCT, WCT, +1>(Z, tw);
+      else if constexpr (NCT > 0)
         Z = fft_ct<NCT, WCT, +1>(Z, other, tw);
       else
         Z = fft_tile<+1>(Z, other, tw, a.plan, W, ln);
     }
     fence_async_shared();
     __syncthreads();
-    stored_wk = Z == Wk;
+    stored_wk = !INPL && Z == Wk;
     if (threadIdx.x == 0) {
       const int x = (int)(2 * c0);
       for (int yb = 0; yb < n; yb += nbox) tma_store_3d(&tout, x, yb, (int)o, Z + (size_t)yb * W);
@@ -897,6 +905,22 @@ __global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<
     }
   }
   if (threadIdx.x == 0) bulk_wait_read();
+}
+
+template <typename T, int MODE, int DIM, int NCT = 0, int WCT = 0>
+__global__ void __launch_bounds__(tile_max_threads<NCT, WCT>(), cols_min_blocks<T, MODE, NCT>())
+    cols_tma_kernel(const __grid_constant__ CUtensorMap tin,
+                    const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
+  cols_tma_body<T, MODE, DIM, NCT, WCT, false>(tin, tout, a, nbox);
+}
+
+// Green tiles transformed in place (no partner tile): twice the columns in
+// the same shared memory, every thread busy in the largest-radix stage
+template <typename T, int DIM, int NCT, int WCT>
+__global__ void __launch_bounds__(ct_threads_inplace<NCT, WCT>(), cols_min_blocks<T, 2, NCT>())
+    cols_tma_inplace_kernel(const __grid_constant__ CUtensorMap tin,
+                            const __grid_constant__ CUtensorMap tout, ColsArgs<T> a, int nbox) {
+  cols_tma_body<T, 2, DIM, NCT, WCT, true>(tin, tout, a, nbox);
 }
 
 // y[l][v] = local(v) : x[l][v]; load case l = blockIdx.y; a voxel's CC
@@ -1211,7 +1235,7 @@ int persistent_grid(K kernel, int threads, size_t smem, int64_t tiles) {
 // tile width and shared memory of the tensor-TMA column kernel: two input
 // tiles and one compute partner of n x W complex, 128-byte aligned
 bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem, int* nbuf,
-                    bool stage_ax0, const ColsTuning* tune) {
+                    bool stage_ax0, const ColsTuning* tune, bool inplace = false) {
   const size_t cs = dtype == F64 ? 16 : 8;
   // built-in rule, measured on B200 (128^3 x 6, FP64): W = 8 columns for
   // plain passes, 12 (two 6-component coefficients) for the Green pass
@@ -1219,8 +1243,10 @@ bool cols_tma_shape(int dtype, int n, int unit, int* W, size_t* smem, int* nbuf,
   if (tune && tune->w >= unit && tune->w % unit == 0 && tune->w <= 128) w = tune->w;
   if (w < unit) w = unit;
   // + the axis-0 Green values (4 reals per row, unless tabulated) and alignment
+  // input tiles, plus the transforms' partner tile unless they run in place
   auto bytes_for = [&](int ww, int nb) {
-    return n * cs + (nb + 1) * 128 + (nb + 1) * (size_t)n * ww * cs +
+    const int nt = inplace ? nb : nb + 1;
+    return n * cs + nt * 128 + nt * (size_t)n * ww * cs +
            (stage_ax0 ? (size_t)n * 2 * cs + 128 : 0);
   };
   // a TMA box row must span a multiple of 16 bytes: widths that do not
@@ -1556,6 +1582,19 @@ cudaError_t cols_ct_launch(const CUtensorMap& tin, const CUtensorMap& tout,
   return cudaGetLastError();
 }
 
+template <typename T, int DIM, int N, int W>
+cudaError_t cols_inplace_launch(const CUtensorMap& tin, const CUtensorMap& tout,
+                                const ColsArgs<T>& a, int nbox, size_t smem, int64_t tiles,
+                                cudaStream_t st) {
+  auto k = &cols_tma_inplace_kernel<T, DIM, N, W>;
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  const int threads = ct_threads_inplace<N, W>();
+  const int grid = persistent_grid(k, threads, smem, tiles);
+  k<<<grid, threads, smem, st>>>(tin, tout, a, nbox);
+  return cudaGetLastError();
+}
+
 template <typename T, int N>
 cudaError_t cols_ct_dispatch(int mode, int dim, const CUtensorMap& tin, const CUtensorMap& tout,
                              const ColsArgs<T>& a, int nbox, size_t smem, int64_t tiles,
@@ -1615,6 +1654,37 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     int Wp, nbuf;
     size_t sp;
     const size_t cs = sizeof(cx<T>);
+    // Green tiles transformed in place: 24 columns at n = 128, 12 at n = 256,
+    // where that width fits.  Tuning value ct = 2 asks for them; the built-in
+    // rule (no schedule set) takes them for 3D grids at n = 256 and in FP32
+    // at n = 128 (measured on B200, 128^3 x 6 and 256^3 x 2: Green pass FP64
+    // 256: -17%, FP32 256: -8%, FP32 128: -5%, FP64 128: equal)
+    const bool rule = !tune || (tune->w == 0 && tune->nbuf == 0 && tune->ct == 1);
+    const bool want_inplace =
+        (tune && tune->ct == 2) || (rule && dim == 3 && (n == 256 || sizeof(T) == 4));
+    if (mode == 2 && want_inplace && (n == 128 || n == 256) && (C == 3 || C == 6) &&
+        al16(in) && al16(out) && (a.pitch * cs) % 16 == 0) {
+      const int wi = n == 128 ? 24 : 12;
+      ColsTuning ti = tune ? *tune : ColsTuning{};
+      ti.w = wi;
+      if (cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, C, &Wp, &sp, &nbuf, a.mn == nullptr, &ti,
+                         true) &&
+          Wp == wi) {
+        CUtensorMap tin, tout;
+        if (make_cols_map(&tin, in, sizeof(T) == 8, inner, a.pitch, n, outer, Wp, n) &&
+            make_cols_map(&tout, out, sizeof(T) == 8, inner, a.pitch, n, outer, Wp, n)) {
+          ColsArgs<T> b = a;
+          b.W = Wp;
+          b.nbuf = nbuf;
+          const int64_t tiles = (inner + Wp - 1) / Wp * outer;
+          if (n == 128)
+            return dim == 2 ? cols_inplace_launch<T, 2, 128, 24>(tin, tout, b, n, sp, tiles, st)
+                            : cols_inplace_launch<T, 3, 128, 24>(tin, tout, b, n, sp, tiles, st);
+          return dim == 2 ? cols_inplace_launch<T, 2, 256, 12>(tin, tout, b, n, sp, tiles, st)
+                          : cols_inplace_launch<T, 3, 256, 12>(tin, tout, b, n, sp, tiles, st);
+        }
+      }
+    }
     // rows 16-byte aligned; a last chunk reaching past `inner` is zero-filled
     // by the load and clipped by the store
     if (al16(in) && al16(out) && (a.pitch * cs) % 16 == 0 &&

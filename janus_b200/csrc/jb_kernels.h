@@ -130,7 +130,9 @@ cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const v
 // tile schedule of a column pass (0 = the built-in rule): tile width in
 // complex columns (a multiple of the coefficient size for the Green pass),
 // rotating input tiles (2 or 3), and whether compile-time FFT tiles may be
-// used where they exist.  Chosen per operator by the autotuner.
+// used where they exist (0 no, 1 yes, 2 Green tiles transformed in place:
+// 24 columns at n = 128, 12 at n = 256, no partner tile).  Chosen per
+// operator by the autotuner.
 struct ColsTuning {
   int w = 0;
   int nbuf = 0;
