@@ -881,6 +881,23 @@ def run_kernels(args, rank):
                 _gradient(cell, r.eps, r.eps.clone())
                 calls.append(tag + " local gradient")
             torch.cuda.synchronize()
+    # the 256-point tiles (rows, plain columns, in-place Green columns): one
+    # truncated-operator basic-scheme iteration on one 256^3 field per precision
+    shape = (256, 256, 256)
+    phase = (rng.random(shape) < 0.3).astype(np.uint8)
+    mat0 = material.create(50.5, 0.3, 3)
+    pars = [(3 * (material.create(g, nu, 3).k - mat0.k), 2 * (g - 50.5))
+            for g, nu in ((1.0, 0.3), (100.0, 0.2))]
+    tens = [ops.isotropic_4(a, b, 3) for a, b in pars]
+    for dt in (torch.float64, torch.float32):
+        loc = ops.BlockDiagonalOperator3D.from_phases(phase, tens, dtype=dt)
+        g = truncated(mat0.green_operator(), shape, 1.0, dtype=dt)
+        BasicScheme(g, loc, nload=1).run(np.eye(6)[:1], 1)
+        calls.append("3D 256^3/{} basic scheme (truncated)".format(
+            "f64" if dt == torch.float64 else "f32"))
+        del loc, g
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
     print(json.dumps({"workload": "kernels", "calls": calls}), flush=True)
 
 
