@@ -124,9 +124,15 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.thread.join(timeout=5)
+        return self.summarise(self.lines)
+
+    @staticmethod
+    def summarise(lines):
+        """Median SM clock, the largest max clock and the throttle reasons seen
+        active in nvidia-smi CSV lines of FIELDS (None without a sample)."""
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 8:
                 continue

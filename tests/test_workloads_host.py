@@ -47,3 +47,23 @@ def test_bench_byte_model_is_the_algorithmic_one():
     # 11 s p + m per 3D voxel-iteration (FP64: 529 B, FP32: 265 B)
     assert sum(bench.pass_bytes(6, 8).values()) == 529
     assert sum(bench.pass_bytes(6, 4).values()) == 265
+
+
+def test_clock_summary_from_nvidia_smi_lines():
+    lines = ["1965, 1965, 812.3, 0x0000000000000000, Not Active, Not Active, Not Active, "
+             "Not Active",
+             "1950, 1965, 990.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+             "1965, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+             "[N/A], 1965, 0, 0x0, Not Active, Not Active, Not Active, Not Active",
+             "garbage"]
+    s = bench.ClockSampler.summarise(lines)
+    assert s == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"],
+                 "samples": 3}
+    assert bench.ClockSampler.summarise([]) is None
+
+
+def test_measured_peak_reads_the_file_or_falls_back(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.measured_peak() == (bench.FALLBACK_HBM_GBS, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 6558.4, "bf16_tflops": 1590}')
+    assert bench.measured_peak() == (6558.4, "measured")
