@@ -67,3 +67,24 @@ def test_measured_peak_reads_the_file_or_falls_back(tmp_path, monkeypatch):
     assert bench.measured_peak() == (bench.FALLBACK_HBM_GBS, "fallback")
     (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 6558.4, "bf16_tflops": 1590}')
     assert bench.measured_peak() == (6558.4, "measured")
+
+
+def test_reference_arm_line_on_a_small_cell():
+    """The reference arm (the reference's own CPU path, one process per load
+    case) prints the contract's JSON line; run here on a 16^3 cell."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.abspath(bench.__file__))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "1", "--n", "16"],
+                         capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["unit"] == "voxel-iter/s" and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"],
+                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
