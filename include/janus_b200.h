@@ -137,12 +137,14 @@ int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
  * compile-time tiles allowed}; widths in complex columns (the Green one a
  * multiple of s), input tiles 2 or 3, 0 = built-in rule; a Green
  * compile-time value of 2 transforms the Green tiles in place (24 columns at
- * n = 128, 12 at n = 256, no partner tile).  A width whose
- * tiles do not fit the shared-memory budget is narrowed.  An optional 7th
- * value selects the Green contraction: 0 built-in rule (the M/N table for
- * the filtered operator, on the fly for the truncated and finite-difference
- * ones), 1 the M/N table, 2 on the fly.  Set by the autotuner
- * (janus_b200.autotune) from timed candidates; count is 6 or 7. */
+ * n = 128, 12 at n = 256, no partner tile), 3 takes the Green pass whose
+ * middle radix-4 stage and contraction run in registers (n0 = 32, 64, 128;
+ * also the built-in rule there).  A width whose tiles do not fit the
+ * shared-memory budget is narrowed.  An optional 7th value selects the Green
+ * contraction: 0 built-in rule (the table for the filtered operator, on the
+ * fly for the truncated and finite-difference ones), 1 the table of
+ * per-coefficient symmetric Mandel matrices, 2 on the fly.  Set by the
+ * autotuner (janus_b200.autotune) from timed candidates; count is 6 or 7. */
 int jb_green_set_tuning(jb_green *green, const int *v, int count);
 int jb_green_get_tuning(jb_green *green, int *v, int count);
 /* set_frequency + to_memoryview at index b (green.pyx:146-171, 312-342 and

@@ -7,8 +7,10 @@ n = 64, 128, 256; runtime mixed-radix plans otherwise); what is tuned is how
 the column passes tile the spectrum: the width of a tile in complex columns,
 how many input tiles rotate through shared memory, whether the compile-time
 tiles are used (for the Green pass also in place, without a partner tile,
-24 columns wide at n = 128 and 12 at n = 256), and whether the Green contraction reads the per-coefficient
-M/N table or evaluates the operator on the fly.  Each candidate is timed on the solver step it
+24 columns wide at n = 128 and 12 at n = 256, or the pass whose middle
+radix-4 stage and contraction run in registers, n0 = 32, 64, 128), and
+whether the Green contraction reads the per-coefficient table of symmetric
+Mandel matrices or evaluates the operator on the fly.  Each candidate is timed on the solver step it
 will serve (CUDA events around every pass, several steps after a warm-up),
 the plain passes (3D axis 1) and the Green pass independently, and the
 fastest of each is set on the operator.  Results are cached per GPU model,
@@ -41,7 +43,7 @@ def get_tuning(green_op):
 
 def set_tuning(green_op, values):
     """6 values (schedules) or 7 (with the contraction mode: 0 rule, 1
-    M/N table, 2 on the fly)."""
+    table, 2 on the fly)."""
     values = [int(x) for x in values]
     v = (ctypes.c_int * len(values))(*values)
     _lib.check(_lib.lib().jb_green_set_tuning(green_op.handle, v, len(values)))
@@ -54,8 +56,10 @@ def candidates(dim, dtype):
     green = [(w, nb, 1) for w in (s, 2 * s, 3 * s) for nb in (2, 3)] + [(s, 2, 0),
                                                                           (2 * s, 2, 0)]
     # tiles transformed in place: 24 columns at n = 128, 12 at n = 256 (other
-    # lengths run these as ordinary compile-time or runtime-plan tiles)
-    green += [(24, 2, 2), (12, 2, 2)]
+    # lengths run these as ordinary compile-time or runtime-plan tiles); the
+    # pass with its middle radix-4 stage in registers (n0 = 32, 64, 128; its
+    # tile is fixed; other lengths run the compile-time tiles)
+    green += [(24, 2, 2), (12, 2, 2), (0, 0, 3)]
     return (plain if dim == 3 else []), green
 
 
@@ -117,7 +121,7 @@ def tune(green_op, local_op, nload=1, steps=5, warmup=2, use_cache=True):
         ms = sum(t.get(p, 0.0) for p in _PLAIN_PASSES)
         if ms < best_plain[1]:
             best_plain = (list(c), ms)
-    for mode in (1, 2):   # M/N table, on the fly
+    for mode in (1, 2):   # table, on the fly
         for c in green_c:
             set_tuning(green_op, best_plain[0] + list(c) + [mode])
             t = _time_passes(solver, eps, res, steps, warmup)

@@ -254,9 +254,9 @@ struct jb_green_s {
   std::vector<void*> tables;
   DeviceBuf spec;
   DeviceBuf bidx;
-  DeviceBuf mnbuf;        // per-coefficient M/N table, built on first use
+  DeviceBuf mnbuf;        // per-coefficient operator table, built on first use
   jb::ColsTuning tune_plain, tune_green;  // column-pass schedules (autotuner)
-  int tune_table = 0;  // Green contraction: 0 built-in rule, 1 M/N table, 2 on the fly
+  int tune_table = 0;  // Green contraction: 0 built-in rule, 1 table, 2 on the fly
   bool use_table = true;  // false: evaluate the operator on the fly
 };
 
@@ -325,7 +325,7 @@ int upload_table(jb_green* g, int dtype, const std::vector<double>& v, void** ou
 
 // spectral passes shared by jb_green_apply and the solver
 // x: real fields (or eps with local), spec: complex scratch, y: output
-// whether the Green pass contracts through the M/N table (else on the fly):
+// whether the Green pass contracts through the table (else on the fly):
 // the tuned choice, or the built-in rule (the table for the filtered
 // operator's 2^d aliases per coefficient, on the fly for one alias)
 bool green_uses_table(const jb_green* g) {
@@ -333,14 +333,14 @@ bool green_uses_table(const jb_green* g) {
          (g->tune_table == 1 || (g->tune_table == 0 && g->variant == JB_FILTERED));
 }
 
-// the operator's M/N tensors at every half-spectrum coefficient, built once
+// the operator's symmetric Mandel matrix at every half-spectrum coefficient, built once
 // on first use (or ahead of a graph capture)
 int green_prepare(jb_green* g, cudaStream_t st) {
   if (!g->use_table || g->gt.mn) return JB_OK;
   const int dim = g->dim;
   const int64_t n0 = g->n[0], n1 = g->n[1];
   const int64_t m = (dim == 2 ? g->n[1] : g->n[2]) / 2 + 1;
-  const int NT = dim == 3 ? 21 : 8;
+  const int NT = dim == 3 ? 21 : 6;
   const size_t bytes = (size_t)n0 * (dim == 3 ? n1 * m : m) * NT * real_size(g->dtype);
   JB_TRY(ensure_buf(g->mnbuf, bytes));
   JB_TRY(launch_status(jb::launch_green_table(g->dtype, dim, g->gt, n0, n1, m, g->mnbuf.p, st),
@@ -391,7 +391,7 @@ int green_passes(jb_green* g, const void* x, void* y, int64_t L, void* spec,
     rec->mark(st);
   }
   const int64_t inner0 = (dim == 2 ? m : n1 * m) * C;
-  // the contraction reads the M/N table (built once) or evaluates the
+  // the contraction reads the table (built once) or evaluates the
   // operator on the fly; built-in rule: the table for the filtered operator
   // (2^d aliases per coefficient), on the fly for the single-alias ones
   const bool table = green_uses_table(g);
@@ -710,8 +710,9 @@ int jb_green_set_tuning(jb_green* G, const int* v, int count) {
     return fail(JB_EINVAL, "tile widths must be in [0, 128], the Green one a multiple of s");
   for (int k : {v[1], v[4]})
     if (k != 0 && k != 2 && k != 3) return fail(JB_EINVAL, "input tiles must be 0, 2 or 3");
-  if (v[5] < 0 || v[5] > 2)
-    return fail(JB_EINVAL, "Green compile-time value must be 0, 1 or 2 (in place)");
+  if (v[5] < 0 || v[5] > 3)
+    return fail(JB_EINVAL,
+                "Green compile-time value must be 0, 1, 2 (in place) or 3 (register radix-4)");
   G->tune_plain.w = v[0];
   G->tune_plain.nbuf = v[1];
   G->tune_plain.ct = v[2] != 0;

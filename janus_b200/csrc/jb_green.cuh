@@ -373,9 +373,24 @@ __device__ __forceinline__ void mn_build(int variant, const T* a0, const T* a1, 
   }
 }
 
-// te <- M te + te M - N:te (Mandel, real and imaginary parts)
-template <int DIM, typename T, typename C>
-__device__ __forceinline__ void mn_apply(const T* mn, C* te) {
+// ---------------------------------------------------------------------------
+// Tabulated operator: the symmetric Mandel matrix G of the discrete operator
+// at one coefficient (o = G t for the real and the imaginary part), upper
+// triangle stored diagonal first:
+//   3D (21): G00 G11 G22 G33 G44 G55 | G01 G02 G03 G04 G05 G12 G13 G14 G15
+//            G23 G24 G25 G34 G35 G45
+//   2D (6):  G00 G11 G22 | G01 G02 G12
+// The reference applies the filtered operator as this matrix too
+// (green.pyx:954-973, 687-694).  Column J is the M/N contraction of the
+// Mandel unit vector e_J, so the table carries the same sums as the M/N form.
+// ---------------------------------------------------------------------------
+template <int DIM> struct GSize;
+template <> struct GSize<2> { static constexpr int value = 6; };
+template <> struct GSize<3> { static constexpr int value = 21; };
+
+// o = (M t + t M - N:t) for one real Mandel vector t
+template <int DIM, typename T>
+__device__ __forceinline__ void mn_apply_real(const T* mn, const T* t, T* o) {
   const T u = T(0.70710678118654752440084436210485);
   const T s2 = T(1.4142135623730950488016887242097);
   if (DIM == 3) {
@@ -383,56 +398,95 @@ __device__ __forceinline__ void mn_apply(const T* mn, C* te) {
     const T n400 = mn[6], n040 = mn[7], n004 = mn[8], n220 = mn[9], n202 = mn[10],
             n022 = mn[11], n310 = mn[12], n301 = mn[13], n130 = mn[14], n031 = mn[15],
             n103 = mn[16], n013 = mn[17], n211 = mn[18], n121 = mn[19], n112 = mn[20];
-#pragma unroll
-    for (int part = 0; part < 2; ++part) {
-      const T t00 = part ? te[0].y : te[0].x;
-      const T t11 = part ? te[1].y : te[1].x;
-      const T t22 = part ? te[2].y : te[2].x;
-      const T t12 = u * (part ? te[3].y : te[3].x);
-      const T t20 = u * (part ? te[4].y : te[4].x);
-      const T t01 = u * (part ? te[5].y : te[5].x);
-      const T S00 = n400 * t00 + n220 * t11 + n202 * t22 + T(2) * (n211 * t12 + n301 * t20 + n310 * t01);
-      const T S11 = n220 * t00 + n040 * t11 + n022 * t22 + T(2) * (n031 * t12 + n121 * t20 + n130 * t01);
-      const T S22 = n202 * t00 + n022 * t11 + n004 * t22 + T(2) * (n013 * t12 + n103 * t20 + n112 * t01);
-      const T S12 = n211 * t00 + n031 * t11 + n013 * t22 + T(2) * (n022 * t12 + n112 * t20 + n121 * t01);
-      const T S20 = n301 * t00 + n121 * t11 + n103 * t22 + T(2) * (n112 * t12 + n202 * t20 + n211 * t01);
-      const T S01 = n310 * t00 + n130 * t11 + n112 * t22 + T(2) * (n121 * t12 + n211 * t20 + n220 * t01);
-      const T P00 = T(2) * (m00 * t00 + m01 * t01 + m20 * t20);
-      const T P11 = T(2) * (m01 * t01 + m11 * t11 + m12 * t12);
-      const T P22 = T(2) * (m20 * t20 + m12 * t12 + m22 * t22);
-      const T P12 = (m11 + m22) * t12 + m12 * (t11 + t22) + m01 * t20 + m20 * t01;
-      const T P20 = (m22 + m00) * t20 + m20 * (t22 + t00) + m12 * t01 + m01 * t12;
-      const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11) + m20 * t12 + m12 * t20;
-      const T o0 = P00 - S00, o1 = P11 - S11, o2 = P22 - S22;
-      const T o3 = s2 * (P12 - S12), o4 = s2 * (P20 - S20), o5 = s2 * (P01 - S01);
-      if (part == 0) {
-        te[0].x = o0; te[1].x = o1; te[2].x = o2; te[3].x = o3; te[4].x = o4; te[5].x = o5;
-      } else {
-        te[0].y = o0; te[1].y = o1; te[2].y = o2; te[3].y = o3; te[4].y = o4; te[5].y = o5;
-      }
-    }
+    const T t00 = t[0], t11 = t[1], t22 = t[2];
+    const T t12 = u * t[3], t20 = u * t[4], t01 = u * t[5];
+    const T S00 = n400 * t00 + n220 * t11 + n202 * t22 + T(2) * (n211 * t12 + n301 * t20 + n310 * t01);
+    const T S11 = n220 * t00 + n040 * t11 + n022 * t22 + T(2) * (n031 * t12 + n121 * t20 + n130 * t01);
+    const T S22 = n202 * t00 + n022 * t11 + n004 * t22 + T(2) * (n013 * t12 + n103 * t20 + n112 * t01);
+    const T S12 = n211 * t00 + n031 * t11 + n013 * t22 + T(2) * (n022 * t12 + n112 * t20 + n121 * t01);
+    const T S20 = n301 * t00 + n121 * t11 + n103 * t22 + T(2) * (n112 * t12 + n202 * t20 + n211 * t01);
+    const T S01 = n310 * t00 + n130 * t11 + n112 * t22 + T(2) * (n121 * t12 + n211 * t20 + n220 * t01);
+    const T P00 = T(2) * (m00 * t00 + m01 * t01 + m20 * t20);
+    const T P11 = T(2) * (m01 * t01 + m11 * t11 + m12 * t12);
+    const T P22 = T(2) * (m20 * t20 + m12 * t12 + m22 * t22);
+    const T P12 = (m11 + m22) * t12 + m12 * (t11 + t22) + m01 * t20 + m20 * t01;
+    const T P20 = (m22 + m00) * t20 + m20 * (t22 + t00) + m12 * t01 + m01 * t12;
+    const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11) + m20 * t12 + m12 * t20;
+    o[0] = P00 - S00;
+    o[1] = P11 - S11;
+    o[2] = P22 - S22;
+    o[3] = s2 * (P12 - S12);
+    o[4] = s2 * (P20 - S20);
+    o[5] = s2 * (P01 - S01);
   } else {
     const T m00 = mn[0], m11 = mn[1], m01 = mn[2];
     const T n40 = mn[3], n31 = mn[4], n22 = mn[5], n13 = mn[6], n04 = mn[7];
-#pragma unroll
-    for (int part = 0; part < 2; ++part) {
-      const T t00 = part ? te[0].y : te[0].x;
-      const T t11 = part ? te[1].y : te[1].x;
-      const T t01 = u * (part ? te[2].y : te[2].x);
-      const T S00 = n40 * t00 + n22 * t11 + T(2) * n31 * t01;
-      const T S11 = n22 * t00 + n04 * t11 + T(2) * n13 * t01;
-      const T S01 = n31 * t00 + n13 * t11 + T(2) * n22 * t01;
-      const T P00 = T(2) * (m00 * t00 + m01 * t01);
-      const T P11 = T(2) * (m01 * t01 + m11 * t11);
-      const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11);
-      const T o0 = P00 - S00, o1 = P11 - S11, o2 = s2 * (P01 - S01);
-      if (part == 0) {
-        te[0].x = o0; te[1].x = o1; te[2].x = o2;
-      } else {
-        te[0].y = o0; te[1].y = o1; te[2].y = o2;
-      }
-    }
+    const T t00 = t[0], t11 = t[1], t01 = u * t[2];
+    const T S00 = n40 * t00 + n22 * t11 + T(2) * n31 * t01;
+    const T S11 = n22 * t00 + n04 * t11 + T(2) * n13 * t01;
+    const T S01 = n31 * t00 + n13 * t11 + T(2) * n22 * t01;
+    const T P00 = T(2) * (m00 * t00 + m01 * t01);
+    const T P11 = T(2) * (m01 * t01 + m11 * t11);
+    const T P01 = (m00 + m11) * t01 + m01 * (t00 + t11);
+    o[0] = P00 - S00;
+    o[1] = P11 - S11;
+    o[2] = s2 * (P01 - S01);
   }
+}
+
+// G from the M/N tensors of one coefficient (column J = contraction of e_J;
+// the upper triangle is kept)
+template <int DIM, typename T>
+__device__ __forceinline__ void mn_to_g(const T* mn, T* g) {
+  constexpr int S = DIM == 3 ? 6 : 3;
+  T col[S][S];
+#pragma unroll
+  for (int j = 0; j < S; ++j) {
+    T e[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) e[i] = i == j ? T(1) : T(0);
+    mn_apply_real<DIM, T>(mn, e, col[j]);
+  }
+  int q = 0;
+#pragma unroll
+  for (int i = 0; i < S; ++i) g[q++] = col[i][i];
+#pragma unroll
+  for (int i = 0; i < S; ++i)
+#pragma unroll
+    for (int j = i + 1; j < S; ++j) g[q++] = col[j][i];
+}
+
+// o = G t for one real Mandel vector (G in the table order above)
+template <int DIM, typename T>
+__device__ __forceinline__ void g_apply_real(const T* g, const T* t, T* o) {
+  if (DIM == 3) {
+    o[0] = g[0] * t[0] + g[6] * t[1] + g[7] * t[2] + g[8] * t[3] + g[9] * t[4] + g[10] * t[5];
+    o[1] = g[6] * t[0] + g[1] * t[1] + g[11] * t[2] + g[12] * t[3] + g[13] * t[4] + g[14] * t[5];
+    o[2] = g[7] * t[0] + g[11] * t[1] + g[2] * t[2] + g[15] * t[3] + g[16] * t[4] + g[17] * t[5];
+    o[3] = g[8] * t[0] + g[12] * t[1] + g[15] * t[2] + g[3] * t[3] + g[18] * t[4] + g[19] * t[5];
+    o[4] = g[9] * t[0] + g[13] * t[1] + g[16] * t[2] + g[18] * t[3] + g[4] * t[4] + g[20] * t[5];
+    o[5] = g[10] * t[0] + g[14] * t[1] + g[17] * t[2] + g[19] * t[3] + g[20] * t[4] + g[5] * t[5];
+  } else {
+    o[0] = g[0] * t[0] + g[3] * t[1] + g[4] * t[2];
+    o[1] = g[3] * t[0] + g[1] * t[1] + g[5] * t[2];
+    o[2] = g[4] * t[0] + g[5] * t[1] + g[2] * t[2];
+  }
+}
+
+// te <- G te (real and imaginary parts)
+template <int DIM, typename T, typename C>
+__device__ __forceinline__ void g_apply(const T* g, C* te) {
+  constexpr int S = DIM == 3 ? 6 : 3;
+  T re[S], im[S], ore[S], oim[S];
+#pragma unroll
+  for (int i = 0; i < S; ++i) {
+    re[i] = te[i].x;
+    im[i] = te[i].y;
+  }
+  g_apply_real<DIM, T>(g, re, ore);
+  g_apply_real<DIM, T>(g, im, oim);
+#pragma unroll
+  for (int i = 0; i < S; ++i) te[i] = mkc(ore[i], oim[i]);
 }
 
 // Per-axis values of one index b_d: truncated k (slot 0) or the filtered

@@ -602,7 +602,7 @@ template <typename T> struct ColsArgs {
   int W, C;
   int64_t m_last;
   GreenTables<T> gt;
-  const T* mn;  // MODE 2: M/N table, or nullptr to evaluate the operator on the fly
+  const T* mn;  // MODE 2: operator table (symmetric Mandel matrices), or nullptr: on the fly
   int nbuf;     // tensor-TMA kernel: rotating input tiles (2 or 3)
 };
 
@@ -778,7 +778,7 @@ __device__ __forceinline__ void cols_tma_body(const CUtensorMap& tin, const CUte
     for (int i = threadIdx.x; i < n; i += blockDim.x) ax0[i] = axis_values(a.gt, 0, i);
   __syncthreads();
   // tile t -> (o, chunk); the Green pass walks the load cases of a chunk
-  // consecutively so they share its M/N table slice in L2
+  // consecutively so they share its table slice in L2
   auto tile_of = [&](int64_t t, int64_t& o, int64_t& chunk) {
     if (MODE == 2) {
       chunk = t / a.outer;
@@ -823,9 +823,9 @@ __device__ __forceinline__ void cols_tma_body(const CUtensorMap& tin, const CUte
     use += nb == 0;
     buf = nb;
     if (MODE == 2 && a.mn != nullptr) {
-      // the tile's M/N slice ([f][c][e], consecutive coefficients adjacent)
-      // heads for L1 while the forward transform runs
-      constexpr int NT = MnSize<DIM>::value;
+      // the tile's table slice ([f][c][e], consecutive coefficients
+      // adjacent) heads for L1 while the forward transform runs
+      constexpr int NT = GSize<DIM>::value;
       const int nf = (Wc + a.C - 1) / a.C;
       const char* base = reinterpret_cast<const char*>(a.mn + (size_t)(c0 / a.C) * n * NT);
       const int lines = (int)(((size_t)nf * n * NT * sizeof(T) + 127) / 128);
@@ -869,13 +869,13 @@ __device__ __forceinline__ void cols_tma_body(const CUtensorMap& tin, const CUte
             b2 = 0;
           }
           if (a.mn != nullptr) {
-            constexpr int NT = MnSize<DIM>::value;
+            constexpr int NT = GSize<DIM>::value;
             const T* tab = a.mn + (size_t)f * n * NT;
             for (int e = e0; e < n; e += est) {
-              T mn[NT];
+              T g[NT];
 #pragma unroll
-              for (int c = 0; c < NT; ++c) mn[c] = __ldg(tab + (size_t)c * n + e);
-              mn_apply<DIM, T>(mn, Z + e * W + col0);
+              for (int c = 0; c < NT; ++c) g[c] = __ldg(tab + (size_t)c * n + e);
+              g_apply<DIM, T>(g, Z + e * W + col0);
             }
           } else {
             const AxisK<T> a1 = axis_values(a.gt, 1, b1);
@@ -1052,7 +1052,8 @@ __global__ void axpy_f32_to_f64_kernel(int64_t n, const float* __restrict__ d,
 template <typename T, int DIM>
 __global__ void green_table_kernel(GreenTables<T> gt, int64_t n0, int64_t n1, int64_t m_last,
                                    T* out) {
-  constexpr int NT = MnSize<DIM>::value;
+  constexpr int NM = MnSize<DIM>::value;
+  constexpr int NT = GSize<DIM>::value;
   const int64_t f12n = DIM == 3 ? n1 * m_last : m_last;
   const int64_t total = f12n * n0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
@@ -1069,10 +1070,11 @@ __global__ void green_table_kernel(GreenTables<T> gt, int64_t n0, int64_t n1, in
     const AxisK<T> a0 = axis_values(gt, 0, b0);
     const AxisK<T> a1 = axis_values(gt, 1, b1);
     const AxisK<T> a2 = DIM == 3 ? axis_values(gt, 2, b2) : a1;
-    T mn[NT];
+    T mn[NM], g[NT];
     mn_build<DIM, T>(gt.variant, a0.v, a1.v, a2.v, gt.inv2g, gt.c1, mn);
+    mn_to_g<DIM, T>(mn, g);
 #pragma unroll
-    for (int c = 0; c < NT; ++c) out[(f * NT + c) * n0 + b0] = mn[c];
+    for (int c = 0; c < NT; ++c) out[(f * NT + c) * n0 + b0] = g[c];
   }
 }
 
@@ -1660,6 +1662,16 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     // at n = 128 (measured on B200, 128^3 x 6 and 256^3 x 2: Green pass FP64
     // 256: -17%, FP32 256: -8%, FP32 128: -5%, FP64 128: equal)
     const bool rule = !tune || (tune->w == 0 && tune->nbuf == 0 && tune->ct == 1);
+    // the register radix-4 Green pass (n = 32, 64, 128): tuning value ct = 3,
+    // and the built-in rule wherever it exists
+    if (mode == 2 && gt && green_axis0_r4_supported(n, C, dim) &&
+        ((tune && tune->ct == 3) || rule)) {
+      GreenDeviceTables g2 = *gt;
+      g2.mn = a.mn;
+      const cudaError_t e = launch_green_axis0_r4(sizeof(T) == 8 ? F64 : F32, ax, outer, inner,
+                                                  a.pitch, in, out, C, dim, g2, m_last, st);
+      if (e != cudaErrorNotSupported) return e;
+    }
     const bool want_inplace =
         (tune && tune->ct == 2) || (rule && dim == 3 && (n == 256 || sizeof(T) == 4));
     if (mode == 2 && want_inplace && (n == 128 || n == 256) && (C == 3 || C == 6) &&

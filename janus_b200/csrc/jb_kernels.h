@@ -27,7 +27,7 @@ struct GreenDeviceTables {
   void* wp[3] = {nullptr, nullptr, nullptr};
   double inv2g = 0, c1 = 0;
   int variant = 0;
-  const void* mn = nullptr;  // per-coefficient M/N table (T), built by launch_green_table
+  const void* mn = nullptr;  // per-coefficient operator table (T), built by launch_green_table
 };
 
 // Real-side geometry of a batch of fields [L][rows][n][C] with arbitrary
@@ -131,7 +131,8 @@ cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const v
 // complex columns (a multiple of the coefficient size for the Green pass),
 // rotating input tiles (2 or 3), and whether compile-time FFT tiles may be
 // used where they exist (0 no, 1 yes, 2 Green tiles transformed in place:
-// 24 columns at n = 128, 12 at n = 256, no partner tile).  Chosen per
+// 24 columns at n = 128, 12 at n = 256, no partner tile; 3 the Green pass
+// with its middle radix-4 stage in registers, n = 32, 64, 128).  Chosen per
 // operator by the autotuner.
 struct ColsTuning {
   int w = 0;
@@ -148,9 +149,20 @@ cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
                         cudaStream_t st, const ColsTuning* tune = nullptr,
                         int64_t pitch = 0);
-// M/N table of the Green operator on the half spectrum of an n0 x n1 (x n2)
-// grid: table[(f12 * n0 + b0) * NT + c], f12 = b1 * m + b2 (3D) or b1 (2D),
-// NT = 21 (3D) / 8 (2D).  `out` has n0 * n1 * m * NT (3D) reals of the dtype.
+// Axis-0 Green pass for n0 = 32, 64, 128 with the middle radix-4 stage and
+// the contraction in registers (jb_green_axis0.cu): in/out complex
+// [L][n0][pitch] (the first `inner` = F * C of each row), in place allowed;
+// gt.mn, when set, is the operator table of launch_green_table.
+bool green_axis0_r4_supported(int n0, int C, int dim);
+cudaError_t launch_green_axis0_r4(int dtype, const AxisData& ax0, int64_t L, int64_t inner,
+                                  int64_t pitch, const void* in, void* out, int C, int dim,
+                                  const GreenDeviceTables& gt, int64_t m_last,
+                                  cudaStream_t st);
+// Table of the Green operator on the half spectrum of an n0 x n1 (x n2) grid:
+// the symmetric Mandel matrix of each coefficient, upper triangle (order in
+// jb_green.cuh, GSize), component-major: table[(f12 * NT + c) * n0 + b0],
+// f12 = b1 * m + b2 (3D) or b1 (2D), NT = 21 (3D) / 6 (2D).  `out` has
+// n0 * n1 * m * NT (3D) reals of the dtype.
 cudaError_t launch_green_table(int dtype, int dim, const GreenDeviceTables& gt, int64_t n0,
                                int64_t n1, int64_t m_last, void* out, cudaStream_t st);
 // y[l][v] = (C - C0)(v) : x[l][v] on a phase map (contiguous fields)
