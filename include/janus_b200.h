@@ -38,6 +38,19 @@ extern "C" {
 #define JB_ECUDA (-2)    /* CUDA runtime error */
 #define JB_ENOMEM (-3)   /* device allocation failed */
 #define JB_ESTATE (-4)   /* call not valid in the handle's state */
+#define JB_EFAULT (-5)   /* a kernel gave up a bounded wait for an asynchronous copy
+                            (device fault word set): this call's results are invalid */
+
+/* Per-load-case outcome of a solve (status[] of the run calls below).  No
+ * counterpart in the reference, whose tutorial loop only records the
+ * residuals (sphinx/tutorials/square_basic/square_basic.py:88-92).  A load
+ * case stops taking part in the stopping test as soon as it is
+ * non-finite or diverging; the call returns once every load case has
+ * converged or stopped, or at the iteration limit. */
+#define JB_SOLVE_CONVERGED 0   /* residual <= tol */
+#define JB_SOLVE_MAX_ITER 1    /* iteration limit reached above tol */
+#define JB_SOLVE_NON_FINITE 2  /* a residual was NaN or infinite */
+#define JB_SOLVE_DIVERGING 3   /* a residual grew 1e4-fold over the smallest one seen */
 
 #define JB_F64 0
 #define JB_F32 1
@@ -64,6 +77,13 @@ int jb_max_axis_length(int dtype);
  * skipped its tile (no reference counterpart; the reference has no device
  * code).  Synchronises with the device. */
 int jb_device_status(unsigned *fault);
+/* Polls of the first bounded wait of every asynchronous copy in the pass
+ * kernels (0 restores the default, 2^24).  For tests of the failure path
+ * only: a small value makes the first wait give up while the copy is still
+ * in flight; the kernel then sets the fault word, waits at the full limit
+ * for its own copy and returns, and the solvers report JB_EFAULT at their
+ * next synchronisation.  No reference counterpart. */
+int jb_set_wait_limit(unsigned polls);
 
 /* ---- real FFT objects ------------------------------------------------- */
 
@@ -213,14 +233,16 @@ int jb_solver_create(jb_green *green, jb_local *local, int nload,
                      jb_solver **out);
 int jb_solver_destroy(jb_solver *solver);
 /* eps: device T[nload][grid][s]; E: host double[nload][s]. If init != 0,
- * eps is set to E first.  Runs until every load case has res <= tol or
- * max_iter iterations.  residuals: host double[max_iter][nload] (may be
- * NULL); iters_out: iterations done; mean_tau: host double[nload][s], the
- * grid mean of (C - C0):eps at the final eps (may be NULL).  The call
- * returns after the work on `stream` has completed. */
+ * eps is set to E first.  Runs until every load case has res <= tol (or has
+ * stopped, non-finite or diverging) or max_iter iterations.  residuals: host
+ * double[max_iter][nload] (may be NULL); iters_out: iterations done;
+ * mean_tau: host double[nload][s], the grid mean of (C - C0):eps at the
+ * final eps (may be NULL); status: host int[nload], JB_SOLVE_* (may be
+ * NULL).  The device fault word is read at every iteration (JB_EFAULT).
+ * The call returns after the work on `stream` has completed. */
 int jb_solver_run(jb_solver *solver, const double *E, void *eps, int init,
                   int max_iter, double tol, double *residuals, int *iters_out,
-                  double *mean_tau, void *stream);
+                  double *mean_tau, int *status, void *stream);
 /* Set the macroscopic strains E (host double[nload][s]) used by
  * jb_solver_step. */
 int jb_solver_set_load(jb_solver *solver, const double *E);
@@ -246,11 +268,13 @@ int jb_gmres_destroy(jb_gmres *solver);
  * the true residual at each restart, or after max_iter Arnoldi steps.
  * residuals: host double[max_iter][nload], the Givens estimate of each step
  * (may be NULL); iters_out: Arnoldi steps done; final_residuals: host
- * double[nload], the true residual at exit (may be NULL); mean_tau as for
- * jb_solver_run.  Returns after the work on `stream` has completed. */
+ * double[nload], the true residual at exit (may be NULL); mean_tau and
+ * status as for jb_solver_run (a load case whose residual estimate is not
+ * finite stops).  Returns after the work on `stream` has completed. */
 int jb_gmres_run(jb_gmres *solver, const double *E, void *eps, int init,
                  int max_iter, double tol, double *residuals, int *iters_out,
-                 double *final_residuals, double *mean_tau, void *stream);
+                 double *final_residuals, double *mean_tau, int *status,
+                 void *stream);
 
 /* ---- mixed-precision basic scheme (defect correction) ------------------- */
 
@@ -281,12 +305,13 @@ int jb_mixed_destroy(jb_mixed *solver);
 int jb_mixed_set_method(jb_mixed *solver, int method);
 /* eps: device double[nload][grid][s]; E host double[nload][s]; residuals:
  * host double[max_outer][nload] (FP64 residual at each outer step, may be
- * NULL); outer_out / fp32_iters_out: counts done.  Returns after the work on
+ * NULL); outer_out / fp32_iters_out: counts done; status: host int[nload],
+ * JB_SOLVE_* of the FP64 residual (may be NULL).  Returns after the work on
  * `stream` has completed. */
 int jb_mixed_run(jb_mixed *solver, const double *E, void *eps, int init,
                  int max_outer, int inner, double tol, double *residuals,
                  int *outer_out, int *fp32_iters_out, double *mean_tau,
-                 void *stream);
+                 int *status, void *stream);
 
 /* Batched mixed-precision solves (no reference counterpart): `count`
  * problems, each a jb_mixed solver of its own grid (sizes may differ) and
@@ -300,7 +325,9 @@ int jb_mixed_run(jb_mixed *solver, const double *E, void *eps, int init,
  * pointers (FP64 fields [L_p][grid_p][s_p]); residuals host
  * double[max_outer][L_p] per problem (may be NULL); outer_out /
  * fp32_iters_out int[count]; mean_tau host double[L_p][s_p] (may be NULL);
- * graph_launches_out: graph launches made.  The handles are borrowed. */
+ * graph_launches_out: graph launches made; status host int[L_p] per
+ * problem, JB_SOLVE_* (may be NULL; a problem leaves the iteration when all
+ * its load cases have converged or stopped).  The handles are borrowed. */
 typedef struct jb_batch_s jb_batch;
 int jb_batch_create(int count, jb_mixed *const *problems, int branches,
                     jb_batch **out);
@@ -308,7 +335,7 @@ int jb_batch_destroy(jb_batch *batch);
 int jb_batch_run(jb_batch *batch, const double *E, void *const *eps, int init,
                  int max_outer, int inner, double tol, double *residuals,
                  int *outer_out, int *fp32_iters_out, double *mean_tau,
-                 int *graph_launches_out, void *stream);
+                 int *graph_launches_out, int *status, void *stream);
 
 /* Benchmark support: record CUDA events around every pass of the next
  * `max_steps` calls of jb_solver_step (on their stream). */

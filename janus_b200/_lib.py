@@ -16,11 +16,15 @@ from . import build as _build
 
 JB_OK = 0
 JB_EINVAL = -1
+JB_EFAULT = -5
 JB_F64 = 0
 JB_F32 = 1
 JB_TRUNCATED = 0
 JB_FILTERED = 1
 JB_WILLOT = 2
+
+# per-load-case outcome of a solve (status arrays of the run calls)
+SOLVE_STATUS = {0: "converged", 1: "max_iter", 2: "non_finite", 3: "diverging"}
 
 _lock = threading.Lock()
 _lib = None
@@ -39,6 +43,7 @@ _SIGS = {
     "jb_last_error": ([], ctypes.c_char_p),
     "jb_max_axis_length": ([c_int], c_int),
     "jb_device_status": ([ctypes.POINTER(ctypes.c_uint)], c_int),
+    "jb_set_wait_limit": ([ctypes.c_uint], c_int),
     "jb_fft_create": ([c_int, P_int64, c_int, ctypes.c_uint, ctypes.POINTER(c_void_p)], c_int),
     "jb_fft_destroy": ([c_void_p], c_int),
     "jb_fft_r2c": ([c_void_p, c_void_p, P_int64, c_void_p, c_void_p], c_int),
@@ -72,11 +77,12 @@ _SIGS = {
                         c_int),
     "jb_batch_destroy": ([c_void_p], c_int),
     "jb_batch_run": ([c_void_p, P_double, ctypes.POINTER(c_void_p), c_int, c_int, c_int,
-                      c_double, P_double, P_int, P_int, P_double, P_int, c_void_p], c_int),
+                      c_double, P_double, P_int, P_int, P_double, P_int, P_int, c_void_p],
+                     c_int),
     "jb_solver_create": ([c_void_p, c_void_p, c_int, ctypes.POINTER(c_void_p)], c_int),
     "jb_solver_destroy": ([c_void_p], c_int),
     "jb_solver_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_double, P_double, P_int,
-                       P_double, c_void_p], c_int),
+                       P_double, P_int, c_void_p], c_int),
     "jb_solver_set_load": ([c_void_p, P_double], c_int),
     "jb_solver_step": ([c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "jb_solver_timing_begin": ([c_void_p, c_int], c_int),
@@ -88,9 +94,9 @@ _SIGS = {
     "jb_gmres_create": ([c_void_p, c_void_p, c_int, c_int, ctypes.POINTER(c_void_p)], c_int),
     "jb_gmres_destroy": ([c_void_p], c_int),
     "jb_gmres_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_double, P_double, P_int,
-                      P_double, P_double, c_void_p], c_int),
+                      P_double, P_double, P_int, c_void_p], c_int),
     "jb_mixed_run": ([c_void_p, P_double, c_void_p, c_int, c_int, c_int, c_double, P_double,
-                      P_int, P_int, P_double, c_void_p], c_int),
+                      P_int, P_int, P_double, P_int, c_void_p], c_int),
 }
 
 
@@ -131,6 +137,25 @@ def device_status() -> int:
     v = ctypes.c_uint(0)
     check(lib().jb_device_status(ctypes.byref(v)))
     return v.value
+
+
+def check_device(what: str = "janus_b200") -> None:
+    """Raise RuntimeError if a kernel gave up a bounded wait since the last
+    check (the fault word is read and cleared; synchronises the device)."""
+    f = device_status()
+    if f & 1:
+        raise RuntimeError(f"{what}: a kernel gave up a bounded wait for its asynchronous "
+                           f"copies (device fault word {f}); its results are invalid")
+
+
+def set_wait_limit(polls: int) -> None:
+    """Polls of the first bounded wait of every asynchronous copy (0: the
+    default).  For tests of the failure path."""
+    check(lib().jb_set_wait_limit(int(polls)))
+
+
+def status_names(status) -> list:
+    return [SOLVE_STATUS.get(int(v), str(int(v))) for v in status]
 
 
 def i64_array(values):

@@ -87,21 +87,25 @@ class BatchedMixedScheme:
         outer = (ctypes.c_int * P)()
         fp32 = (ctypes.c_int * P)()
         mean = np.zeros(E_all.shape[0])
+        status = np.zeros(sum(sizes), dtype=np.int32)
         launches = ctypes.c_int(0)
         Pd = ctypes.POINTER(ctypes.c_double)
         _lib.check(_lib.lib().jb_batch_run(
             self._handle, E_all.ctypes.data_as(Pd), ptrs, int(init), max_outer, inner,
             float(tol), res.ctypes.data_as(Pd), outer, fp32, mean.ctypes.data_as(Pd),
-            ctypes.byref(launches), ctypes.c_void_p(A.stream_handle())))
+            ctypes.byref(launches), status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            ctypes.c_void_p(A.stream_handle())))
         self.graph_launches = launches.value
         out = []
-        r0 = m0 = 0
+        r0 = m0 = s0 = 0
         for i, s in enumerate(self.schemes):
             L, C = s.nload, s.green_op.ishape[-1]
             hist = res[r0:r0 + max_outer * L].reshape(max_outer, L)[:outer[i]].copy()
             out.append(MixedResult(eps=eps[i], residuals=hist, outer_iterations=outer[i],
                                    fp32_iterations=fp32[i],
-                                   mean_tau=mean[m0:m0 + L * C].reshape(L, C).copy()))
+                                   mean_tau=mean[m0:m0 + L * C].reshape(L, C).copy(),
+                                   status=status[s0:s0 + L].copy()))
             r0 += max_outer * L
             m0 += L * C
+            s0 += L
         return out

@@ -3,8 +3,9 @@
 //
 // Every copy lands in the issuing CTA's own shared memory (no copy is shared
 // across the CTAs of a cluster).  Every wait is bounded: after
-// kWaitLimit polls the kernel records a timeout in g_jb_fault (read by
-// jb_device_status on the host), waits once more (bounded) for its own
+// c_jb_wait_first polls (kWaitLimit by default) the kernel records a timeout
+// in g_jb_fault (read by the solvers at each host synchronisation and by
+// jb_device_status), waits once more, at most kWaitLimit polls, for its own
 // copies, and the caller returns without touching the tile.
 #pragma once
 
@@ -20,6 +21,11 @@ namespace jb {
 __device__ unsigned int g_jb_fault = 0;
 
 constexpr unsigned kWaitLimit = 1u << 24;
+
+// polls of the first bounded wait (kWaitLimit unless lowered through
+// jb_set_wait_limit to exercise the failure path in tests; the drain wait
+// after a timeout always keeps kWaitLimit)
+__constant__ unsigned c_jb_wait_first = kWaitLimit;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -56,7 +62,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // bounded wait for phase `parity` of the barrier; false on timeout (and the
 // fault bit is set)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (unsigned i = 0; i < kWaitLimit; ++i)
+  const unsigned first = c_jb_wait_first;
+  for (unsigned i = 0; i < first; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   atomicOr(&g_jb_fault, 1u);
   for (unsigned i = 0; i < kWaitLimit; ++i)

@@ -147,6 +147,52 @@ int launch_status(cudaError_t e, const char* what) {
   return fail(JB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Outcome of each load case of a solve, updated at every residual readback:
+// a non-finite residual or one grown kDivergeFactor-fold over the smallest
+// seen stops the load case for good (JB_SOLVE_NON_FINITE / _DIVERGING).
+constexpr double kDivergeFactor = 1e4;
+
+struct Outcome {
+  std::vector<double> best, last;
+  std::vector<int> stopped;  // 0, JB_SOLVE_NON_FINITE or JB_SOLVE_DIVERGING
+  explicit Outcome(int L) : best(L, INFINITY), last(L, INFINITY), stopped(L, 0) {}
+  // record residual r of load case l; true when the case no longer holds the
+  // iteration back (converged or stopped)
+  bool update(int l, double r, double tol) {
+    if (stopped[l]) return true;
+    last[l] = r;
+    if (!std::isfinite(r)) {
+      stopped[l] = JB_SOLVE_NON_FINITE;
+      return true;
+    }
+    if (r > tol && best[l] > 0.0 && r > kDivergeFactor * best[l]) {
+      stopped[l] = JB_SOLVE_DIVERGING;
+      return true;
+    }
+    best[l] = std::min(best[l], r);
+    return r <= tol;
+  }
+  void write(double tol, int* status, int off = 0) const {
+    if (!status) return;
+    for (size_t l = 0; l < stopped.size(); ++l)
+      status[off + l] = stopped[l]       ? stopped[l]
+                        : last[l] <= tol ? JB_SOLVE_CONVERGED
+                                         : JB_SOLVE_MAX_ITER;
+  }
+};
+
+// after a stream synchronisation: the fault word fetched with it
+// (fetch_fault_async) must be clear, else the call's results are invalid
+int check_fault(unsigned fetched, const char* what) {
+  if (fetched == 0) return JB_OK;
+  unsigned f = 0;
+  jb::read_and_clear_fault(&f);
+  return fail(JB_EFAULT, std::string(what) +
+                             ": a kernel gave up a bounded wait for its asynchronous copies "
+                             "(device fault word " + std::to_string(fetched) +
+                             "); the results of this call are invalid");
+}
+
 // ---------------------------------------------------------------------------
 // continuous Green operator, isotropic.pyx:158-182 / 227-290, same operations
 // ---------------------------------------------------------------------------
@@ -453,6 +499,11 @@ int jb_max_axis_length(int dtype) { return jb::max_axis_length(dtype); }
 int jb_device_status(unsigned* fault) {
   if (!fault) return fail(JB_EINVAL, "NULL argument");
   JB_CUDA(jb::read_and_clear_fault(fault));
+  return JB_OK;
+}
+
+int jb_set_wait_limit(unsigned polls) {
+  JB_CUDA(jb::set_first_wait_limit(polls));
   return JB_OK;
 }
 
@@ -1163,7 +1214,8 @@ const char* jb_solver_pass_name(jb_solver* S, int i) {
 }
 
 int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_iter, double tol,
-                  double* residuals, int* iters_out, double* mean_tau, void* stream) {
+                  double* residuals, int* iters_out, double* mean_tau, int* status,
+                  void* stream) {
   if (!S || !E || !eps) return fail(JB_EINVAL, "NULL argument");
   if (max_iter < 0) return fail(JB_EINVAL, "max_iter must be >= 0");
   JB_TRY(jb_solver_set_load(S, E));
@@ -1175,16 +1227,20 @@ int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_it
                                                static_cast<const double*>(S->E.p), eps, st),
                          "fill"));
   std::vector<double> r(S->L);
+  Outcome out(S->L);
+  unsigned fault = 0;
   int it = 0;
   for (; it < max_iter; ++it) {
     JB_TRY(jb_solver_step(S, eps, static_cast<double*>(S->res.p), st));
     JB_CUDA(cudaMemcpyAsync(r.data(), S->res.p, sizeof(double) * S->L, cudaMemcpyDeviceToHost,
                             st));
+    JB_CUDA(jb::fetch_fault_async(&fault, st));
     JB_CUDA(cudaStreamSynchronize(st));
+    JB_TRY(check_fault(fault, "jb_solver_run"));
     bool done = true;
     for (int l = 0; l < S->L; ++l) {
       if (residuals) residuals[(size_t)it * S->L + l] = r[l];
-      if (!(r[l] <= tol)) done = false;
+      if (!out.update(l, r[l], tol)) done = false;
     }
     if (done) {
       ++it;
@@ -1192,6 +1248,7 @@ int jb_solver_run(jb_solver* S, const double* E, void* eps, int init, int max_it
     }
   }
   if (iters_out) *iters_out = it;
+  out.write(tol, status);
   if (mean_tau) {
     int nb = 0;
     JB_TRY(launch_status(jb::launch_local_sum(S->green->dtype, local_desc(S->local), C, S->L,
@@ -1314,7 +1371,8 @@ void givens(double a, double b, double& c, double& s) {
 
 extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, int max_iter,
                             double tol, double* residuals, int* iters_out,
-                            double* final_residuals, double* mean_tau, void* stream) {
+                            double* final_residuals, double* mean_tau, int* status,
+                            void* stream) {
   if (!S || !E || !eps) return fail(JB_EINVAL, "NULL argument");
   if (max_iter < 0) return fail(JB_EINVAL, "max_iter must be >= 0");
   if (!(tol >= 0.0)) return fail(JB_EINVAL, "tol must be >= 0");
@@ -1365,6 +1423,7 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
   };
   // one sweep q on w = V_{j+1}: h[l][q (m+1) + i] = V_i . w for i <= j (sweep 0
   // also w . w at i = j + 1), then w -= sum_{i <= j} h_i V_i and sq = |w|^2
+  unsigned fault = 0;
   auto sweep = [&](int j, int q) {
     double* w = V + (int64_t)(j + 1) * vs;
     const int nd = q == 0 ? j + 2 : j + 1;
@@ -1385,10 +1444,12 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     JB_CUDA(cudaMemcpyAsync(hh.data() + (size_t)0, hd, sizeof(double) * L * ldh,
                             cudaMemcpyDeviceToHost, st));
     JB_CUDA(cudaMemcpyAsync(sq.data(), sqd, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
+    JB_CUDA(jb::fetch_fault_async(&fault, st));
     JB_CUDA(cudaStreamSynchronize(st));
-    return JB_OK;
+    return check_fault(fault, "jb_gmres_run");
   };
   std::vector<int> active(L), kuse(L);
+  Outcome out(L);
   int it = 0;
   for (;;) {
     // true residual r = E - A x into V_0
@@ -1396,12 +1457,14 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     JB_TRY(launch_status(jb::launch_gmres_resid(nvox, C, L, Ed, V, V, st), "gmres_resid"));
     JB_TRY(norm2(V));
     JB_CUDA(cudaMemcpyAsync(sq.data(), sqd, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
+    JB_CUDA(jb::fetch_fault_async(&fault, st));
     JB_CUDA(cudaStreamSynchronize(st));
+    JB_TRY(check_fault(fault, "jb_gmres_run"));
     bool done = true;
     for (int l = 0; l < L; ++l) {
       beta[l] = std::sqrt(sq[l]);
       rel[l] = beta[l] / bnorm[l];
-      if (!(rel[l] <= tol)) done = false;
+      if (!out.update(l, rel[l], tol)) done = false;
     }
     if (final_residuals)
       for (int l = 0; l < L; ++l) final_residuals[l] = rel[l];
@@ -1410,7 +1473,10 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     std::fill(g.begin(), g.end(), 0.0);
     for (int l = 0; l < L; ++l) {
       g[(size_t)l * (m + 1)] = beta[l];
-      active[l] = (rel[l] <= tol || !(beta[l] > 0.0) || !std::isfinite(beta[l])) ? 0 : 1;
+      active[l] = (rel[l] <= tol || !(beta[l] > 0.0) || !std::isfinite(beta[l]) ||
+                   out.stopped[l])
+                      ? 0
+                      : 1;
       kuse[l] = 0;
     }
     int j = 0;
@@ -1495,6 +1561,7 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
     }
   }
   if (iters_out) *iters_out = it;
+  out.write(tol, status);
   if (mean_tau) {
     int nb = 0;
     JB_TRY(launch_status(jb::launch_local_sum(F64, loc, C, L, nvox, eps,
@@ -1888,7 +1955,8 @@ int mixed_mean(jb_mixed* M, const void* eps, double* mean_tau, cudaStream_t st) 
 
 extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, int max_outer,
                             int inner, double tol, double* residuals, int* outer_out,
-                            int* fp32_iters_out, double* mean_tau, void* stream) {
+                            int* fp32_iters_out, double* mean_tau, int* status,
+                            void* stream) {
   if (!M || !E || !eps) return fail(JB_EINVAL, "NULL argument");
   if (max_outer < 0) return fail(JB_EINVAL, "max_outer must be >= 0");
   if (inner < 1) return fail(JB_EINVAL, "inner must be >= 1");
@@ -1896,19 +1964,25 @@ extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, i
   const int L = M->L;
   JB_TRY(mixed_set_load(M, E, eps, init, st));
   std::vector<double> r(L);
+  Outcome out(L);
+  unsigned fault = 0;
   int outer = 0, fp32 = 0;
   double rprev = 0.0;  // largest residual of the previous outer step
   int kprev = 0;       // Krylov iterations of the previous correction
   for (; outer < max_outer; ++outer) {
     JB_TRY(mixed_residual(M, eps, static_cast<double*>(M->res.p), st));
     JB_CUDA(cudaMemcpyAsync(r.data(), M->res.p, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
+    JB_CUDA(jb::fetch_fault_async(&fault, st));
     JB_CUDA(cudaStreamSynchronize(st));
+    JB_TRY(check_fault(fault, "jb_mixed_run"));
     bool done = true;
     double rmax = 0.0;
     for (int l = 0; l < L; ++l) {
       if (residuals) residuals[(size_t)outer * L + l] = r[l];
-      if (!(r[l] <= tol)) done = false;
-      rmax = std::max(rmax, r[l]);
+      if (!out.update(l, r[l], tol)) {
+        done = false;
+        rmax = std::max(rmax, r[l]);  // the load cases still iterating
+      }
     }
     if (done) {
       ++outer;
@@ -1938,8 +2012,11 @@ extern "C" int jb_mixed_run(jb_mixed* M, const double* E, void* eps, int init, i
   }
   if (outer_out) *outer_out = outer;
   if (fp32_iters_out) *fp32_iters_out = fp32;
+  out.write(tol, status);
   if (mean_tau) JB_TRY(mixed_mean(M, eps, mean_tau, st));
+  JB_CUDA(jb::fetch_fault_async(&fault, st));
   JB_CUDA(cudaStreamSynchronize(st));
+  JB_TRY(check_fault(fault, "jb_mixed_run"));
   return JB_OK;
 }
 
@@ -2078,7 +2155,7 @@ int batch_capture(jb_batch* B, const std::vector<char>& active, void* const* eps
 extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int init,
                             int max_outer, int inner, double tol, double* residuals,
                             int* outer_out, int* fp32_iters_out, double* mean_tau,
-                            int* graph_launches_out, void* stream) {
+                            int* graph_launches_out, int* status, void* stream) {
   if (!B || !E || !eps) return fail(JB_EINVAL, "NULL argument");
   if (max_outer < 1) return fail(JB_EINVAL, "max_outer must be >= 1");
   if (inner < 1) return fail(JB_EINVAL, "inner must be >= 1");
@@ -2112,11 +2189,18 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
     hist_off[i] = roff;
     roff += (size_t)max_outer * B->prob[i]->L;
   }
+  std::vector<Outcome> outc;
+  outc.reserve(P);
+  for (size_t i = 0; i < P; ++i) outc.emplace_back(B->prob[i]->L);
+  unsigned fault = 0;
   int launches = 0;
   for (int step = 0;; ++step) {
+    cudaStream_t rs = step == 0 ? st : origin;
     JB_CUDA(cudaMemcpyAsync(rh.data(), res, sizeof(double) * B->nres, cudaMemcpyDeviceToHost,
-                            step == 0 ? st : origin));
-    JB_CUDA(cudaStreamSynchronize(step == 0 ? st : origin));
+                            rs));
+    JB_CUDA(jb::fetch_fault_async(&fault, rs));
+    JB_CUDA(cudaStreamSynchronize(rs));
+    JB_TRY(check_fault(fault, "jb_batch_run"));
     bool any = false;
     for (size_t i = 0; i < P; ++i) {
       if (!active[i]) continue;
@@ -2125,7 +2209,7 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
       for (int l = 0; l < L; ++l) {
         const double v = rh[B->res_off[i] + l];
         if (residuals) residuals[hist_off[i] + (size_t)(outer[i] - 1) * L + l] = v;
-        if (!(v <= tol)) done = false;
+        if (!outc[i].update(l, v, tol)) done = false;
       }
       if (done || outer[i] >= max_outer) active[i] = 0;
       any = any || active[i];
@@ -2154,6 +2238,7 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
     jb_mixed* M = B->prob[i];
     const int C = M->g64->dim == 2 ? 3 : 6;
     if (outer_out) outer_out[i] = outer[i];
+    outc[i].write(tol, status, (int)B->res_off[i]);
     if (fp32_iters_out)
       fp32_iters_out[i] =
           (outer[i] - 1) * (M->method != JB_INNER_BASIC ? 2 * inner : inner - 1);

@@ -1741,6 +1741,16 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
 
 int max_axis_length(int dtype) { return dtype == F64 ? 4096 : 8192; }
 
+cudaError_t fetch_fault_async(unsigned* host, cudaStream_t st) {
+  return cudaMemcpyFromSymbolAsync(host, g_jb_fault, sizeof(unsigned), 0,
+                                   cudaMemcpyDeviceToHost, st);
+}
+
+cudaError_t set_first_wait_limit(unsigned polls) {
+  const unsigned v = polls ? polls : kWaitLimit;
+  return cudaMemcpyToSymbol(c_jb_wait_first, &v, sizeof(unsigned));
+}
+
 cudaError_t read_and_clear_fault(unsigned* out) {
   unsigned zero = 0;
   cudaError_t e = cudaMemcpyFromSymbol(out, g_jb_fault, sizeof(unsigned));

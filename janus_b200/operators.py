@@ -302,6 +302,10 @@ class _AbstractStructuredOperator:
         xd = A.to_device(x, self._dtype)
         out = A.Output(y, self._oshape, self._dtype, x)
         self._apply_device(xd, out.target)
+        if out.host:
+            # the result goes back to the host (a synchronisation anyway):
+            # a kernel that gave up a bounded wait invalidates it
+            _lib.check_device(type(self).__name__ + ".apply")
         return out.finish()
 
 

@@ -26,12 +26,27 @@ from . import _lib
 from .operators import LocalPhaseOperator, _BlockDiagonalOperator
 
 
+class _Outcome:
+    """Per-load-case outcome (``status``: ints, 0 converged, 1 max_iter,
+    2 non_finite, 3 diverging; no counterpart in the reference, whose loop
+    records residuals only)."""
+
+    @property
+    def status_names(self):
+        return _lib.status_names(self.status)
+
+    @property
+    def converged(self):
+        return bool(np.all(self.status == 0))
+
+
 @dataclass
-class SolveResult:
+class SolveResult(_Outcome):
     eps: torch.Tensor          # (nload,) + grid + (s,) on the device
     residuals: np.ndarray      # (iterations, nload)
     iterations: int
     mean_tau: np.ndarray       # (nload, s): grid mean of (C - C0):eps
+    status: np.ndarray = None  # (nload,) int32, see _Outcome
 
     def mean_stress(self, mat0, avg_eps):
         """<sigma> = C0:E + <tau> (square_basic.py:95-96, Mandel form)."""
@@ -108,13 +123,16 @@ class BasicScheme:
         res = np.zeros((max(int(num_iter), 1), self.nload))
         it = ctypes.c_int(0)
         mean = np.zeros((self.nload, self.green_op.ishape[-1]))
+        status = np.zeros(self.nload, dtype=np.int32)
         P = ctypes.POINTER(ctypes.c_double)
         _lib.check(_lib.lib().jb_solver_run(
             self._handle, E.ctypes.data_as(P), ctypes.c_void_p(eps.data_ptr()), int(bool(init)),
             int(num_iter), float(tol), res.ctypes.data_as(P), ctypes.byref(it),
-            mean.ctypes.data_as(P), ctypes.c_void_p(A.stream_handle())))
+            mean.ctypes.data_as(P), status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            ctypes.c_void_p(A.stream_handle())))
         n = it.value
-        return SolveResult(eps=eps, residuals=res[:n].copy(), iterations=n, mean_tau=mean)
+        return SolveResult(eps=eps, residuals=res[:n].copy(), iterations=n, mean_tau=mean,
+                           status=status)
 
     def set_load(self, avg_eps):
         E = self._macro(avg_eps)
@@ -152,12 +170,13 @@ def basic_scheme(green_op, local_op, avg_eps, num_iter, tol=0.0, eps=None):
 
 
 @dataclass
-class MixedResult:
+class MixedResult(_Outcome):
     eps: torch.Tensor          # (nload,) + grid + (s,), FP64 on the device
     residuals: np.ndarray      # (outer steps, nload): FP64 residual at each outer step
     outer_iterations: int
     fp32_iterations: int
     mean_tau: np.ndarray       # (nload, s)
+    status: np.ndarray = None  # (nload,) int32, see _Outcome
 
     def mean_stress(self, mat0, avg_eps):
         return _c0_apply(mat0, np.atleast_2d(avg_eps)) + self.mean_tau
@@ -235,25 +254,28 @@ class MixedScheme:
         outer = ctypes.c_int(0)
         fp32 = ctypes.c_int(0)
         mean = np.zeros((self.nload, self.green_op.ishape[-1]))
+        status = np.zeros(self.nload, dtype=np.int32)
         P = ctypes.POINTER(ctypes.c_double)
         _lib.check(_lib.lib().jb_mixed_run(self._handle, E.ctypes.data_as(P),
                                            ctypes.c_void_p(eps.data_ptr()),
                                            int(init), int(max_outer), inner, float(tol),
                                            res.ctypes.data_as(P), ctypes.byref(outer),
                                            ctypes.byref(fp32), mean.ctypes.data_as(P),
+                                           status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                            ctypes.c_void_p(A.stream_handle())))
         n = outer.value
         return MixedResult(eps=eps, residuals=res[:n].copy(), outer_iterations=n,
-                           fp32_iterations=fp32.value, mean_tau=mean)
+                           fp32_iterations=fp32.value, mean_tau=mean, status=status)
 
 
 @dataclass
-class GMRESResult:
+class GMRESResult(_Outcome):
     eps: torch.Tensor          # (nload,) + grid + (s,), FP64 on the device
     residuals: np.ndarray      # (iterations, nload): Givens estimate after each Arnoldi step
     final_residuals: np.ndarray  # (nload,): true residual at exit
     iterations: int            # Arnoldi steps (operator applications besides restarts)
     mean_tau: np.ndarray       # (nload, s)
+    status: np.ndarray = None  # (nload,) int32, see _Outcome
 
     def mean_stress(self, mat0, avg_eps):
         return _c0_apply(mat0, np.atleast_2d(avg_eps)) + self.mean_tau
@@ -316,15 +338,17 @@ class GMRES:
         final = np.zeros(self.nload)
         it = ctypes.c_int(0)
         mean = np.zeros((self.nload, self.green_op.ishape[-1]))
+        status = np.zeros(self.nload, dtype=np.int32)
         P = ctypes.POINTER(ctypes.c_double)
         _lib.check(_lib.lib().jb_gmres_run(
             self._handle, E.ctypes.data_as(P), ctypes.c_void_p(eps.data_ptr()),
             int(bool(init)), int(max_iter), float(tol), res.ctypes.data_as(P),
             ctypes.byref(it), final.ctypes.data_as(P), mean.ctypes.data_as(P),
+            status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
             ctypes.c_void_p(A.stream_handle())))
         n = it.value
         return GMRESResult(eps=eps, residuals=res[:n].copy(), final_residuals=final,
-                           iterations=n, mean_tau=mean)
+                           iterations=n, mean_tau=mean, status=status)
 
 
 class LippmannSchwingerOperator:
