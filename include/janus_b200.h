@@ -284,8 +284,11 @@ int jb_gmres_run(jb_gmres *solver, const double *E, void *eps, int init,
  * r = E - eps - Gamma0[(C - C0):eps] and its norm (the stopping test, same
  * normalisation as jb_solver_run), then runs `inner - 1` FP32 iterations of
  * d <- r - Gamma0[(C - C0):d] from d = r, and adds d to the FP64 eps.
- * g64/l64 and g32/l32 are the same operators built with JB_F64 and JB_F32.
- * The handles are borrowed and must outlive the solver. */
+ * g64/l64 and g32/l32 are the same operators built with JB_F64 and JB_F32;
+ * g32/l32 may also be JB_F64 operators (the FP64 ones themselves), which
+ * runs the same algorithm with FP64 corrections (a control that separates
+ * the inner solver's gain from precision's).  The handles are borrowed and
+ * must outlive the solver. */
 typedef struct jb_mixed_s jb_mixed;
 int jb_mixed_create(jb_green *g64, jb_local *l64, jb_green *g32, jb_local *l32,
                     int nload, jb_mixed **out);

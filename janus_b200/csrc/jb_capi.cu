@@ -1732,6 +1732,7 @@ struct jb_mixed_s {
   jb_local* l32 = nullptr;
   int L = 1;
   int method = JB_INNER_BASIC;
+  int idt = F32;  // precision of the inner (correction) operators and fields
   DeviceBuf spec, partials, E, res, normd, r32, d32, mean;
   DeviceBuf kr_rh, kr_p, kr_v, kr_s, kr_t, kr_r, kr_part, kr_state;  // BiCGSTAB
   std::vector<double> norm;
@@ -1742,8 +1743,9 @@ extern "C" int jb_mixed_create(jb_green* g64, jb_local* l64, jb_green* g32, jb_l
   if (!out) return fail(JB_EINVAL, "out must not be NULL");
   *out = nullptr;
   if (!g64 || !l64 || !g32 || !l32) return fail(JB_EINVAL, "NULL argument");
-  if (g64->dtype != F64 || l64->dtype != F64 || g32->dtype != F32 || l32->dtype != F32)
-    return fail(JB_EINVAL, "jb_mixed_create needs FP64 and FP32 operator pairs");
+  if (g64->dtype != F64 || l64->dtype != F64 || g32->dtype != l32->dtype)
+    return fail(JB_EINVAL, "jb_mixed_create needs FP64 outer operators and inner operators "
+                           "of one precision");
   if (nload < 1 || nload > 65535) return fail(JB_EINVAL, "nload must be in [1, 65535]");
   const int dim = g64->dim;
   if (g32->dim != dim || l64->dim != dim || l32->dim != dim)
@@ -1760,6 +1762,7 @@ extern "C" int jb_mixed_create(jb_green* g64, jb_local* l64, jb_green* g32, jb_l
   M->g32 = g32;
   M->l32 = l32;
   M->L = nload;
+  M->idt = g32->dtype;
   const int C = dim == 2 ? 3 : 6;
   const int64_t nvox = l64->nvox;
   const int64_t rows = dim == 2 ? g64->n[0] : g64->n[0] * g64->n[1];
@@ -1770,8 +1773,8 @@ extern "C" int jb_mixed_create(jb_green* g64, jb_local* l64, jb_green* g32, jb_l
   if (r == JB_OK) r = ensure_buf(M->res, sizeof(double) * nload);
   if (r == JB_OK) r = ensure_buf(M->normd, sizeof(double) * nload);
   if (r == JB_OK) r = ensure_buf(M->mean, sizeof(double) * nload * C);
-  if (r == JB_OK) r = ensure_buf(M->r32, sizeof(float) * nload * nvox * C);
-  if (r == JB_OK) r = ensure_buf(M->d32, sizeof(float) * nload * nvox * C);
+  if (r == JB_OK) r = ensure_buf(M->r32, real_size(M->idt) * nload * nvox * C);
+  if (r == JB_OK) r = ensure_buf(M->d32, real_size(M->idt) * nload * nvox * C);
   if (r != JB_OK) {
     jb_mixed_destroy(M);
     return r;
@@ -1827,10 +1830,31 @@ int mixed_set_load(jb_mixed* M, const double* E, void* eps, int init, cudaStream
   return JB_OK;
 }
 
-// FP64 residual pass: r32 = E - eps - Gamma0[(C - C0):eps] (FP32), its
-// normalised norms into res_out (device double[L])
+// FP64 residual pass: r32 = E - eps - Gamma0[(C - C0):eps] (in the inner
+// precision), its normalised norms into res_out (device double[L])
 int mixed_residual(jb_mixed* M, void* eps, double* res_out, cudaStream_t st) {
   jb::LocalDesc loc64 = local_desc(M->l64);
+  if (M->idt == F64) {
+    // all-FP64 form: A eps into r, r = E - A eps, |r|^2, then the normalised norm
+    const int C = M->g64->dim == 2 ? 3 : 6;
+    const int64_t nvox = M->l64->nvox;
+    double* r = static_cast<double*>(M->r32.p);
+    double* sq = static_cast<double*>(M->partials.p);
+    jb::UpdateDesc u;
+    u.mode = 4;  // r = eps + Gamma0[(C - C0):eps]
+    u.eps = r;
+    u.rhs = eps;
+    JB_TRY(green_passes(M->g64, eps, r, M->L, M->spec.p, &loc64, &u, nullptr, st));
+    JB_TRY(launch_status(jb::launch_gmres_resid(nvox, C, M->L,
+                                                static_cast<const double*>(M->E.p), r, r, st),
+                         "resid"));
+    JB_TRY(launch_status(jb::launch_gmres_dots(nvox * C, M->L, r, r, 0, 0, 1,
+                                               sq + M->L, sq, 1, 0, st),
+                         "dots"));
+    return launch_status(jb::launch_reduce_rows(sq, M->L, 1, res_out, 1.0,
+                                                static_cast<const double*>(M->normd.p), 1, st),
+                         "reduce");
+  }
   jb::UpdateDesc u;
   u.mode = 2;
   u.eps = eps;
@@ -1851,9 +1875,9 @@ int mixed_correct(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
   const int C = M->g64->dim == 2 ? 3 : 6;
   const int64_t nel = (int64_t)M->L * M->l64->nvox * C;
   jb::LocalDesc loc32 = local_desc(M->l32);
-  float* r32 = static_cast<float*>(M->r32.p);
-  float* d32 = static_cast<float*>(M->d32.p);
-  JB_CUDA(cudaMemcpyAsync(d32, r32, sizeof(float) * nel, cudaMemcpyDeviceToDevice, st));
+  void* r32 = M->r32.p;
+  void* d32 = M->d32.p;
+  JB_CUDA(cudaMemcpyAsync(d32, r32, real_size(M->idt) * nel, cudaMemcpyDeviceToDevice, st));
   for (int j = 1; j < inner; ++j) {
     jb::UpdateDesc v;
     v.mode = 3;
@@ -1861,8 +1885,8 @@ int mixed_correct(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
     v.rhs = r32;
     JB_TRY(green_passes(M->g32, d32, d32, M->L, M->spec.p, &loc32, &v, nullptr, st));
   }
-  return launch_status(jb::launch_axpy_f32_to_f64(nel, d32, static_cast<double*>(eps), st),
-                       "axpy");
+  return launch_status(
+      jb::launch_axpy_to_f64(M->idt, nel, d32, static_cast<double*>(eps), st), "axpy");
 }
 
 // correction by `inner` BiCGSTAB iterations on A d = r (FP32, A d = d +
@@ -1873,7 +1897,7 @@ int mixed_krylov_buffers(jb_mixed* M) {
   const int C = M->g64->dim == 2 ? 3 : 6;
   const int L = M->L;
   const int64_t nel = M->l64->nvox * C;
-  const size_t fb = sizeof(float) * (size_t)L * nel;
+  const size_t fb = real_size(M->idt) * (size_t)L * nel;
   for (DeviceBuf* b : {&M->kr_rh, &M->kr_p, &M->kr_v, &M->kr_s, &M->kr_t, &M->kr_r})
     JB_TRY(ensure_buf(*b, fb));
   JB_TRY(ensure_buf(M->kr_part, sizeof(double) * 2 * L * jb::krylov_blocks(nel, L)));
@@ -1884,14 +1908,14 @@ int mixed_correct_bicgstab(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
   const int C = M->g64->dim == 2 ? 3 : 6;
   const int L = M->L;
   const int64_t nel = M->l64->nvox * C;
-  const size_t fb = sizeof(float) * (size_t)L * nel;
+  const int dt = M->idt;
+  const size_t fb = real_size(dt) * (size_t)L * nel;
   JB_TRY(mixed_krylov_buffers(M));
   jb::LocalDesc loc32 = local_desc(M->l32);
-  float* x = static_cast<float*>(M->d32.p);
-  float* b = static_cast<float*>(M->r32.p);
-  float *rh = static_cast<float*>(M->kr_rh.p), *p = static_cast<float*>(M->kr_p.p),
-        *v = static_cast<float*>(M->kr_v.p), *s = static_cast<float*>(M->kr_s.p),
-        *t = static_cast<float*>(M->kr_t.p), *r = static_cast<float*>(M->kr_r.p);
+  void* x = M->d32.p;
+  void* b = M->r32.p;
+  void *rh = M->kr_rh.p, *p = M->kr_p.p, *v = M->kr_v.p, *s = M->kr_s.p, *t = M->kr_t.p,
+       *r = M->kr_r.p;
   double* part = static_cast<double*>(M->kr_part.p);
   auto* ks = static_cast<jb::KrylovState*>(M->kr_state.p);
   JB_CUDA(cudaMemsetAsync(x, 0, fb, st));
@@ -1899,10 +1923,10 @@ int mixed_correct_bicgstab(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
   JB_CUDA(cudaMemsetAsync(v, 0, fb, st));
   JB_CUDA(cudaMemcpyAsync(r, b, fb, cudaMemcpyDeviceToDevice, st));
   JB_CUDA(cudaMemcpyAsync(rh, b, fb, cudaMemcpyDeviceToDevice, st));
-  JB_TRY(launch_status(jb::launch_krylov_dot(F32, nel, L, rh, r, nullptr, nullptr, part, st),
+  JB_TRY(launch_status(jb::launch_krylov_dot(dt, nel, L, rh, r, nullptr, nullptr, part, st),
                        "krylov_dot"));
   JB_TRY(launch_status(jb::launch_krylov_scalars(0, nel, L, part, ks, st), "krylov_scalars"));
-  auto apply = [&](const float* in, float* out) {
+  auto apply = [&](const void* in, void* out) {
     jb::UpdateDesc u;
     u.mode = 4;  // out = in + Gamma0[(C - C0):in]
     u.eps = out;
@@ -1911,27 +1935,26 @@ int mixed_correct_bicgstab(jb_mixed* M, void* eps, int inner, cudaStream_t st) {
   };
   for (int it = 0; it < inner; ++it) {
     JB_TRY(launch_status(
-        jb::launch_krylov_update(F32, 0, nel, L, p, nullptr, nullptr, v, r, nullptr, ks, nullptr,
+        jb::launch_krylov_update(dt, 0, nel, L, p, nullptr, nullptr, v, r, nullptr, ks, nullptr,
                                  st),
         "krylov_p"));
     JB_TRY(apply(p, v));
-    JB_TRY(launch_status(jb::launch_krylov_dot(F32, nel, L, rh, v, nullptr, nullptr, part, st),
+    JB_TRY(launch_status(jb::launch_krylov_dot(dt, nel, L, rh, v, nullptr, nullptr, part, st),
                          "krylov_dot"));
     JB_TRY(launch_status(jb::launch_krylov_scalars(1, nel, L, part, ks, st), "krylov_scalars"));
     JB_TRY(launch_status(
-        jb::launch_krylov_update(F32, 1, nel, L, s, nullptr, nullptr, v, r, nullptr, ks, nullptr,
+        jb::launch_krylov_update(dt, 1, nel, L, s, nullptr, nullptr, v, r, nullptr, ks, nullptr,
                                  st),
         "krylov_s"));
     JB_TRY(apply(s, t));
-    JB_TRY(launch_status(jb::launch_krylov_dot(F32, nel, L, t, s, t, t, part, st), "krylov_dot"));
+    JB_TRY(launch_status(jb::launch_krylov_dot(dt, nel, L, t, s, t, t, part, st), "krylov_dot"));
     JB_TRY(launch_status(jb::launch_krylov_scalars(2, nel, L, part, ks, st), "krylov_scalars"));
     JB_TRY(launch_status(
-        jb::launch_krylov_update(F32, 2, nel, L, x, p, s, t, r, rh, ks, part, st), "krylov_xr"));
+        jb::launch_krylov_update(dt, 2, nel, L, x, p, s, t, r, rh, ks, part, st), "krylov_xr"));
     JB_TRY(launch_status(jb::launch_krylov_scalars(3, nel, L, part, ks, st), "krylov_scalars"));
   }
-  return launch_status(jb::launch_axpy_f32_to_f64((int64_t)L * nel, x, static_cast<double*>(eps),
-                                                  st),
-                       "axpy");
+  return launch_status(
+      jb::launch_axpy_to_f64(dt, (int64_t)L * nel, x, static_cast<double*>(eps), st), "axpy");
 }
 
 // mean of (C - C0):eps per load case and component into host mean_tau

@@ -1027,6 +1027,24 @@ __global__ void green_by_freq_kernel(GreenTables<T> gt, int64_t count, const int
   }
 }
 
+__global__ void axpy_f64_kernel(int64_t n, const double* __restrict__ d,
+                                double* __restrict__ y) {
+  const int64_t n2 = n / 2;
+  const double2* d2 = reinterpret_cast<const double2*>(d);
+  double2* y2 = reinterpret_cast<double2*>(y);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = d2[i];
+    double2 a = y2[i];
+    a.x += v.x;
+    a.y += v.y;
+    y2[i] = a;
+  }
+  for (int64_t i = 2 * n2 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += d[i];
+}
+
 __global__ void axpy_f32_to_f64_kernel(int64_t n, const float* __restrict__ d,
                                        double* __restrict__ y) {
   const int64_t n4 = n / 4;
@@ -1918,6 +1936,14 @@ cudaError_t launch_fill_macro(int dtype, int C, int L, int64_t nvox, const doubl
     fill_macro_kernel<double><<<grid, kThreads, 0, st>>>(C, L, nvox, E, static_cast<double*>(eps));
   else
     fill_macro_kernel<float><<<grid, kThreads, 0, st>>>(C, L, nvox, E, static_cast<float*>(eps));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy_to_f64(int dtype, int64_t n, const void* d, double* y,
+                               cudaStream_t st) {
+  if (dtype == F32) return launch_axpy_f32_to_f64(n, static_cast<const float*>(d), y, st);
+  if (n <= 0) return cudaSuccess;
+  axpy_f64_kernel<<<grid_for(n / 2 + 1), kThreads, 0, st>>>(n, static_cast<const double*>(d), y);
   return cudaGetLastError();
 }
 

@@ -102,6 +102,8 @@ cudaError_t launch_gmres_scale(int64_t nel, int L, double* w, const double* sq, 
 cudaError_t launch_gmres_resid(int64_t nvox, int C, int L, const double* E, const double* ax,
                                double* r, cudaStream_t st);
 cudaError_t launch_axpy_f32_to_f64(int64_t n, const float* d, double* y, cudaStream_t st);
+// y[i] += d[i], d of the dtype (FP32 or FP64)
+cudaError_t launch_axpy_to_f64(int dtype, int64_t n, const void* d, double* y, cudaStream_t st);
 
 int max_axis_length(int dtype);
 // bit 0: a kernel gave up a bounded wait (see jb_async.cuh); cleared on read

@@ -197,11 +197,14 @@ class MixedScheme:
     the Krylov route of the reference's examples/square_inclusion_scipy.py,
     which hands the same operator to scipy's gmres.  The FP32 operators are
     built from the given FP64 ones (same material, grid, discretisation and
-    phase map)."""
+    phase map).  ``inner_dtype=torch.float64`` runs the same algorithm with
+    FP64 corrections (the given operators serve both levels): the control
+    that separates the gain of the inner solver from that of precision."""
 
     METHODS = {"basic": 0, "bicgstab": 1, "bicgstab_fixed": 2}
 
-    def __init__(self, green_op, local_op, nload=1, inner=20, method="basic"):
+    def __init__(self, green_op, local_op, nload=1, inner=20, method="basic",
+                 inner_dtype=torch.float32):
         if isinstance(local_op, _BlockDiagonalOperator):
             local = local_op.local
         else:
@@ -214,9 +217,15 @@ class MixedScheme:
         self.local = local
         self.nload = int(nload)
         self.inner = int(inner)
-        self.green32 = type(green_op)(green_op.green, green_op.ishape[:-1], green_op.h,
-                                      dtype=torch.float32)
-        self.local32 = local.with_dtype(torch.float32)
+        if inner_dtype == torch.float64:
+            self.green32, self.local32 = green_op, local
+        elif inner_dtype == torch.float32:
+            self.green32 = type(green_op)(green_op.green, green_op.ishape[:-1], green_op.h,
+                                          dtype=torch.float32)
+            self.local32 = local.with_dtype(torch.float32)
+        else:
+            raise ValueError("inner_dtype must be torch.float32 or torch.float64")
+        self.inner_dtype = inner_dtype
         if method not in self.METHODS:
             raise ValueError("method must be 'basic', 'bicgstab' or 'bicgstab_fixed'")
         self.method = method

@@ -132,3 +132,28 @@ def test_mixed_bicgstab_homogeneous_cell_stays_finite():
                                                                         max_outer=5)
     assert np.isfinite(r.eps.cpu().numpy()).all()
     assert np.abs(r.eps.cpu().numpy() - E.reshape(3, 1, 1, 3)).max() <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["basic", "bicgstab"])
+def test_fp64_inner_control_matches_fp64(method):
+    """The same defect correction with FP64 corrections (the precision
+    control): converges to the FP64 basic scheme's solution, and with BiCGSTAB
+    in a handful of outer steps."""
+    import torch
+    phase, _ = micro.random_spheres(32, radius=4, volume_fraction=0.3, seed=5)
+    mats = [(1.0, 0.3), (100.0, 0.2)]
+    g0, nu0 = 50.5, 0.3
+    loc, green, pars = _problem(phase, mats, g0, nu0, "truncated")
+    E = np.eye(6)[[0, 5]]
+    tol = 1e-10
+    ref = BasicScheme(green, loc, nload=2).run(E, 5000, tol=tol)
+    ctl = MixedScheme(green, loc, nload=2, inner=20, method=method,
+                      inner_dtype=torch.float64).run(E, tol=tol, max_outer=500)
+    assert ctl.converged and ctl.residuals[-1].max() <= tol
+    mat0 = material.create(g0, nu0, 3)
+    c_ref = ref.mean_stress(mat0, E)
+    c_ctl = ctl.mean_stress(mat0, E)
+    assert np.abs(c_ctl - c_ref).max() <= 1e-8 * np.abs(c_ref).max()
+    if method == "bicgstab":
+        assert ctl.outer_iterations <= 10
