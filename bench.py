@@ -174,24 +174,71 @@ def build_problem(n, seed, variant, dtype):
 # CPU leg: the reference's serial path (or the oracle port) on one load case
 # ---------------------------------------------------------------------------
 
-def reference_available():
+def reference_available(fftw=None):
     from oracle import reference
-    return reference.load()
+    return reference.load(fftw=fftw)
 
 
-def cpu_worker(n, seed, load, iters, variant, out_path):
+# what the timed CPU baseline runs, by kind
+CPU_LABELS = {
+    "reference": "reference Cython + project FFT shim (not FFTW)",
+    "reference+fftw": "reference Cython + FFTW",
+    "port": "oracle numpy port of the reference (numpy.fft)",
+}
+
+
+def fftw_probe():
+    """Path of a system libfftw3 (double precision), or None, and how it was
+    looked for (ldconfig -p, then the usual library directories)."""
+    found = None
+    try:
+        out = subprocess.run(["ldconfig", "-p"], capture_output=True, text=True,
+                             timeout=10).stdout
+        for line in out.splitlines():
+            if "libfftw3.so.3" in line and "=>" in line:
+                found = line.split("=>")[-1].strip()
+                break
+    except Exception:
+        pass
+    if found is None:
+        for d in ("/usr/lib/x86_64-linux-gnu", "/usr/lib64", "/usr/lib", "/usr/local/lib"):
+            cand = os.path.join(d, "libfftw3.so.3")
+            if os.path.exists(cand):
+                found = cand
+                break
+    info = {"ldconfig_libfftw3": found, "fftw3_h": os.path.exists("/usr/include/fftw3.h")}
+    if found is None:
+        info["fftw"] = "unavailable on this box"
+    return found, info
+
+
+def host_cpu():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count()}
+
+
+def cpu_worker(n, seed, load, iters, variant, out_path, field_path=None, fftw=None):
     """Run `iters` basic-scheme iterations of one load case with the
-    reference's own objects (the tutorial loop, square_basic.py:83-92)."""
+    reference's own objects (the tutorial loop, square_basic.py:83-92);
+    optionally save the last iterate (the parity leg's oracle field)."""
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     import numpy as np
     from janus_b200 import microstructures as micro
     phase, _ = micro.random_spheres(n, radius=8 * n / 128, volume_fraction=0.3, seed=seed)
     E = np.zeros(6)
     E[load] = 1.0
-    ref = reference_available()
+    ref = reference_available(fftw)
     times = []
     if ref is not None:
-        kind = "reference"
+        kind = "reference+fftw" if fftw else "reference"
         import janus.fft.serial as rfft
         import janus.green as rgreen
         import janus.material.elastic.linear.isotropic as rmat
@@ -234,47 +281,63 @@ def cpu_worker(n, seed, load, iters, variant, out_path):
             _ = np.linalg.norm(new - eps)
             eps = new
             times.append(time.perf_counter() - t0)
+    if field_path:
+        np.save(field_path, eps)
     with open(out_path, "w") as f:
         json.dump({"kind": kind, "times": times}, f)
 
 
-def run_cpu_workers(n, seed, loads, iters, variant, tag):
+def run_cpu_workers(n, seed, loads, iters, variant, tag, save_field=False, fftw=None):
     import tempfile
     procs = []
     outs = []
     env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1",
                MKL_NUM_THREADS="1", CUDA_VISIBLE_DEVICES="")
     tmpdir = tempfile.mkdtemp(prefix="jb_cpu_")
+    fields = []
     for load in loads:
         out = os.path.join(tmpdir, f"{tag}_{load}.json")
         outs.append(out)
-        procs.append(subprocess.Popen(
-            [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--n", str(n),
-             "--seed", str(seed), "--load", str(load), "--iters", str(iters),
-             "--variant", variant, "--out", out], env=env))
+        cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--n", str(n),
+               "--seed", str(seed), "--load", str(load), "--iters", str(iters),
+               "--variant", variant, "--out", out]
+        if save_field:
+            fields.append(os.path.join(tmpdir, f"{tag}_{load}_eps.npy"))
+            cmd += ["--field", fields[-1]]
+        if fftw:
+            cmd += ["--fftw", fftw]
+        procs.append(subprocess.Popen(cmd, env=env))
     for p in procs:
         p.wait()
     results = []
-    for p, out in zip(procs, outs):
+    for i, (p, out) in enumerate(zip(procs, outs)):
         if p.returncode != 0 or not os.path.exists(out):
             raise RuntimeError("CPU worker failed")
         with open(out) as f:
             results.append(json.load(f))
+        if save_field:
+            results[-1]["field"] = fields[i]
     return results
 
 
-def cpu_baseline(n, seed, variant, budget_s=20.0):
+def cpu_baseline(n, seed, variant, budget_s=20.0, fftw=None):
     """1-core time of the reference's serial path on one load case:
-    iterations until about `budget_s` of CPU work (at least 2)."""
-    probe = run_cpu_workers(n, seed, [5], 2, variant, "probe")[0]
+    iterations until about `budget_s` of CPU work (at least 2).  The last
+    iterate is kept (``field``, iteration count ``iterations``) for the
+    parity leg."""
+    probe = run_cpu_workers(n, seed, [5], 2, variant, "probe", fftw=fftw)[0]
     per_it = max(probe["times"][1], 1e-3)
     iters = max(2, min(20, int(budget_s / per_it)))
-    res = run_cpu_workers(n, seed, [5], iters + 1, variant, "base")[0]
+    res = run_cpu_workers(n, seed, [5], iters + 1, variant, "base", save_field=True,
+                          fftw=fftw)[0]
     t = sum(res["times"][1:])
     vox = n ** 3
-    return {"value": vox * iters / t, "unit": UNIT, "cores": 1, "kind": res["kind"],
+    return {"value": vox * iters / t, "unit": UNIT, "cores": 1,
+            "kind": "reference" if res["kind"].startswith("reference") else "port",
+            "label": CPU_LABELS[res["kind"]],
             "sample": f"{iters} basic-scheme iterations of one load case (E = xy) at {n}^3, "
-                      "after 1 untimed iteration, single thread"}
+                      "after 1 untimed iteration, single thread",
+            "host_cpu": host_cpu(), "field": res["field"], "iterations": iters + 1}
 
 
 # ---------------------------------------------------------------------------
@@ -400,85 +463,60 @@ def run_gpu(args, rank, world, dist):
                        "pinned host memory; median of 3 repetitions", "parts": parts}
 
     solve = None
-    if not args.no_solve and rank == 0 and world == 1:
+    if not args.no_solve and rank == 0 and world == 1 and args.dtype == "f64":
         import janus_b200.material.elastic.linear.isotropic as material
-        eps2 = solver.new_field()
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        rr = solver.run(E, args.solve_max_iter, tol=args.tol, eps=eps2, init=True)
-        b.record()
-        torch.cuda.synchronize()
-        mat0 = material.create(*REF_MEDIUM, 3)
-        c64 = rr.mean_stress(mat0, E)
-        solve = {"tol": args.tol, "fp64": {
-            "iterations": rr.iterations, "seconds": round(a.elapsed_time(b) / 1e3, 4),
-            "final_residual_max": float(rr.residuals[-1].max()),
-            "C_eff_diag": [float(v) for v in np.diag(c64)]}}
-        if args.dtype == "f64":
-            from janus_b200.solvers import MixedScheme
-            mixed = MixedScheme(green, loc, nload=6, inner=args.inner)
-            eps3 = torch.empty_like(eps2)
-            mixed.run(E, tol=1e-3, max_outer=2, eps=eps3)  # warm the FP32 kernels
-            torch.cuda.synchronize()
-            a.record()
-            rm = mixed.run(E, tol=args.tol, max_outer=args.solve_max_iter)
-            b.record()
-            torch.cuda.synchronize()
-            cm = rm.mean_stress(mat0, E)
-            solve["mixed"] = {
-                "inner": args.inner, "outer_iterations": rm.outer_iterations,
-                "fp32_iterations": rm.fp32_iterations,
-                "seconds": round(a.elapsed_time(b) / 1e3, 4),
-                "final_residual_max": float(rm.residuals[-1].max()),
-                "C_eff_max_rel_diff_vs_fp64": float(np.abs(cm - c64).max() / np.abs(c64).max())}
-            solve["mixed_speedup"] = round(solve["fp64"]["seconds"] / solve["mixed"]["seconds"], 3)
-            # the same defect correction with a Krylov inner solver (BiCGSTAB
-            # on the basic scheme's operator, FP32)
-            kry = MixedScheme(green, loc, nload=6, inner=args.krylov_inner, method="bicgstab")
-            kry.run(E, tol=1e-30, max_outer=2)  # warm: one correction allocates the Krylov fields
-            torch.cuda.synchronize()
-            a.record()
-            rk = kry.run(E, tol=args.tol, max_outer=args.solve_max_iter)
-            b.record()
-            torch.cuda.synchronize()
-            ck = rk.mean_stress(mat0, E)
-            solve["mixed_bicgstab"] = {
-                "inner": args.krylov_inner, "outer_iterations": rk.outer_iterations,
-                "fp32_operator_applications": rk.fp32_iterations,
-                "seconds": round(a.elapsed_time(b) / 1e3, 4),
-                "final_residual_max": float(rk.residuals[-1].max()),
-                "C_eff_max_rel_diff_vs_fp64": float(np.abs(ck - c64).max() / np.abs(c64).max())}
-            solve["mixed_bicgstab_speedup"] = round(
-                solve["fp64"]["seconds"] / solve["mixed_bicgstab"]["seconds"], 3)
-            # FP64 restarted GMRES over the same operator (the reference
-            # examples' Krylov route), same stopping test
-            from janus_b200.solvers import GMRES
-            gm = GMRES(green, loc, nload=6, restart=args.gmres_restart)
-            eps4 = torch.empty_like(eps2)
-            gm.run(E, tol=1e-30, max_iter=2, eps=eps4, init=True)  # warm the kernels
-            torch.cuda.synchronize()
-            a.record()
-            rg = gm.run(E, tol=args.tol, max_iter=args.solve_max_iter, eps=eps4, init=True)
-            b.record()
-            torch.cuda.synchronize()
-            cg = rg.mean_stress(mat0, E)
-            solve["gmres_fp64"] = {
-                "restart": args.gmres_restart, "arnoldi_steps": rg.iterations,
-                "seconds": round(a.elapsed_time(b) / 1e3, 4),
-                "final_residual_max": float(rg.final_residuals.max()),
-                "C_eff_max_rel_diff_vs_fp64": float(np.abs(cg - c64).max() / np.abs(c64).max())}
-            solve["gmres_fp64_speedup"] = round(
-                solve["fp64"]["seconds"] / solve["gmres_fp64"]["seconds"], 3)
-            del gm
+        solve = {"tol": args.tol, "workload": "the bench cell, 6 load cases"}
+        solve.update(time_to_solution(
+            green, loc, E, material.create(*REF_MEDIUM, 3), args.tol, args.inner,
+            args.krylov_inner, args.solve_max_iter,
+            legs=("fp64", "mixed", "mixed_bicgstab", "fp64_bicgstab", "gmres_fp64")))
+        torch.cuda.empty_cache()
+
+    target = None
+    if not args.no_target and rank == 0 and world == 1 and args.dtype == "f64":
+        target = target_leg(args, 2024)
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_baseline(n, 2024, args.variant)
         except Exception as exc:  # pragma: no cover
             cpu = {"value": None, "unit": UNIT, "error": str(exc)}
+        # the reference on real FFTW, where this machine has it
+        fftw_path, fftw_info = fftw_probe()
+        if fftw_path and os.path.isdir(os.path.join(ROOT, "oracle", "_ref_fftw", "janus")):
+            try:
+                cf = cpu_baseline(n, 2024, args.variant, fftw=fftw_path)
+                os.remove(cf.pop("field"))
+                cf.pop("iterations", None)
+                fftw_info["reference_fftw"] = cf
+            except Exception as exc:  # pragma: no cover
+                fftw_info["reference_fftw"] = {"error": str(exc)}
+        elif fftw_path:
+            fftw_info["reference_fftw"] = "no FFTW build of the reference checker (oracle/_ref_fftw)"
+        if cpu.get("value") is not None:
+            cpu["fftw_probe"] = fftw_info
+        # parity: the GPU FP64 iterate after the same iterations of the same
+        # load case against the reference's own field
+        field = cpu.pop("field", None)
+        if field and args.dtype == "f64":
+            import numpy as np
+            ref_eps = np.load(field)
+            os.remove(field)
+            K = cpu.pop("iterations")
+            E5 = np.zeros((1, 6))
+            E5[0, 5] = 1.0
+            r1 = BasicScheme(green, loc, nload=1).run(E5, K)
+            got = r1.eps[0].cpu().numpy()
+            err = float(np.abs(got - ref_eps).max() / np.abs(ref_eps).max())
+            parity = {"max_rel_err": err, "bar": 1e-12, "ok": err <= 1e-12,
+                      "what": f"GPU FP64 basic-scheme iterate after {K} iterations of load "
+                              f"case E = xy at {n}^3 against the {cpu['label']} field of the "
+                              "same iterations (the cpu_baseline run)"}
+            del r1
+        else:
+            cpu.pop("iterations", None)
 
     if rank == 0:
         line = {
@@ -496,7 +534,8 @@ def run_gpu(args, rank, world, dist):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": nrec * len(passes),
             "passes_ms_per_step": {k: round(v / max(nrec, 1), 4) for k, v in passes.items()},
-            "clocks": clocks, "solve": solve, "tuning": tuning,
+            "clocks": clocks, "solve": solve, "target": target, "parity": parity,
+            "tuning": tuning,
         }
         print(json.dumps(line), flush=True)
 
@@ -599,6 +638,116 @@ def run_batch2d(args, rank, world):
                             for p, r in zip(probs, res)], key=lambda v: -v[2])[:16],
     }
     print(json.dumps(line), flush=True)
+
+
+def time_to_solution(green, loc, E, mat0, tol, inner, krylov_inner, max_outer,
+                     legs=("fp64", "mixed", "mixed_bicgstab", "fp64_bicgstab")):
+    """Solve (I + Gamma0 (C - C0)) eps = E to relative residual `tol` with the
+    plain FP64 basic scheme and the defect-correction solvers, CUDA-event
+    timed after a warm-up of each; C_eff of every leg against the FP64 basic
+    scheme's.  Legs: fp64 (basic scheme), mixed (FP32 basic inner sweeps),
+    mixed_bicgstab (FP32 BiCGSTAB inner), fp64_bicgstab (the same BiCGSTAB
+    defect correction in FP64: the control separating the Krylov gain from
+    the precision gain), gmres_fp64 (FP64 restarted GMRES)."""
+    import numpy as np
+    import torch
+
+    from janus_b200.solvers import GMRES, BasicScheme, MixedScheme
+
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    out = {}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b) / 1e3
+
+    fp64 = BasicScheme(green, loc, nload=len(E))
+    fp64.run(E, 3)  # warm (tables, kernels)
+    r64, t64 = timed(lambda: fp64.run(E, max_outer * inner, tol=tol))
+    c64 = r64.mean_stress(mat0, E)
+    del fp64
+    out["fp64"] = {"iterations": r64.iterations, "seconds": round(t64, 4),
+                   "final_residual_max": float(r64.residuals[-1].max()),
+                   "status": r64.status_names}
+
+    def rel(c):
+        return float(np.abs(c - c64).max() / np.abs(c64).max())
+    specs = {"mixed": dict(inner=inner, method="basic"),
+             "mixed_bicgstab": dict(inner=krylov_inner, method="bicgstab"),
+             "fp64_bicgstab": dict(inner=krylov_inner, method="bicgstab",
+                                   inner_dtype=torch.float64)}
+    for leg in legs:
+        if leg in specs:
+            sch = MixedScheme(green, loc, nload=len(E), **specs[leg])
+            sch.run(E, tol=1e-30, max_outer=2)  # warm: kernels, work fields
+            r, t = timed(lambda: sch.run(E, tol=tol, max_outer=max_outer))
+            out[leg] = {"inner": specs[leg]["inner"], "outer_iterations": r.outer_iterations,
+                        "inner_operator_applications": r.fp32_iterations,
+                        "seconds": round(t, 4),
+                        "final_residual_max": float(r.residuals[-1].max()),
+                        "C_eff_max_rel_diff_vs_fp64": rel(r.mean_stress(mat0, E)),
+                        "status": r.status_names}
+            del sch
+        elif leg == "gmres_fp64":
+            gm = GMRES(green, loc, nload=len(E), restart=20)
+            gm.run(E, tol=1e-30, max_iter=2)  # warm
+            r, t = timed(lambda: gm.run(E, tol=tol, max_iter=max_outer * inner))
+            out[leg] = {"restart": 20, "arnoldi_steps": r.iterations, "seconds": round(t, 4),
+                        "final_residual_max": float(r.final_residuals.max()),
+                        "C_eff_max_rel_diff_vs_fp64": rel(r.mean_stress(mat0, E)),
+                        "status": r.status_names}
+            del gm
+        torch.cuda.empty_cache()
+    for leg in list(out):
+        if leg != "fp64":
+            out[leg]["speedup_vs_fp64"] = round(t64 / out[leg]["seconds"], 3)
+    if "fp64_bicgstab" in out and "mixed_bicgstab" in out:
+        # precision alone: the same BiCGSTAB defect correction, FP64 vs FP32 inner
+        out["precision_gain_bicgstab"] = round(
+            out["fp64_bicgstab"]["seconds"] / out["mixed_bicgstab"]["seconds"], 3)
+    if "mixed" in out:
+        out["precision_gain_basic"] = out["mixed"]["speedup_vs_fp64"]
+    out["C_eff_fp64"] = [[float(v) for v in row] for row in c64]
+    return out
+
+
+def target_leg(args, seed):
+    """The time-to-solution target: a seeded 256^3 two-phase periodic
+    Voronoi cell (512 cells, fair-coin phases), mu 1 / 100, nu 0.3,
+    mu0 50.5, truncated Green operator, shear load case, to 1e-8."""
+    import numpy as np
+    import torch
+
+    import janus_b200.material.elastic.linear.isotropic as material
+    from janus_b200 import microstructures as micro
+    from janus_b200 import operators as ops
+    from janus_b200.green import truncated
+
+    n, c, tol = args.target_n, 100.0, 1e-8
+    t0 = time.perf_counter()
+    phase = micro.voronoi(n, cells=512, seed=seed)
+    gen_s = time.perf_counter() - t0
+    mu0, nu0 = 0.5 * (1.0 + c), 0.3
+    mat0 = material.create(mu0, nu0, 3)
+    pars = [(3 * (material.create(g, 0.3, 3).k - mat0.k), 2 * (g - mu0)) for g in (1.0, c)]
+    loc = ops.BlockDiagonalOperator3D.from_phases(phase, [ops.isotropic_4(a, b, 3)
+                                                          for a, b in pars])
+    green = truncated(mat0.green_operator(), (n, n, n), 1.0)
+    E = np.eye(6)[-1:]
+    res = time_to_solution(green, loc, E, mat0, tol, args.inner, args.krylov_inner,
+                           args.solve_max_iter)
+    del loc, green
+    torch.cuda.empty_cache()
+    return {"workload": f"3D two-phase Voronoi {n}^3, 512 cells (seed {seed}), mu 1/{c:g}, "
+                        f"nu 0.3, mu0 {mu0:g}, truncated, E = xy shear, tol {tol:g}",
+            "target": ">= 3x lower time-to-solution than the plain FP64 GPU solver, "
+                      "C_eff within 1e-7 of FP64",
+            "generation_s": round(gen_s, 1), "results": res}
 
 
 def run_voronoi(args, rank):
@@ -926,10 +1075,13 @@ def run_reference(args, rank):
                                f"{args.variant} Green operator, 6 load cases, basic scheme",
                    "grid": [n, n, n], "load_cases": 6, "variant": args.variant,
                    "precision": "f64", "parallelism": "6 single-threaded processes"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 6, "kind": kind,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 6,
+                         "kind": "reference" if kind.startswith("reference") else "port",
+                         "label": CPU_LABELS[kind],
                          "sample": f"{args.steps} timed iterations (after {args.warmup}) of "
                                    f"each of the 6 load cases at {n}^3, one process per load "
-                                   "case (the reference's serial path is single-threaded)"},
+                                   "case (the reference's serial path is single-threaded)",
+                         "host_cpu": host_cpu(), "fftw_probe": fftw_probe()[1]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -983,12 +1135,18 @@ def main(argv=None):
     ap.add_argument("--load", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--iters", type=int, default=1, help=argparse.SUPPRESS)
     ap.add_argument("--out", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--field", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--fftw", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--no-target", action="store_true",
+                    help="skip the time-to-solution target leg (256^3 Voronoi)")
+    ap.add_argument("--target-n", type=int, default=256)
     args = ap.parse_args(argv)
     if args.warmup < 0 or args.steps < 1:
         ap.error("steps must be >= 1 and warmup >= 0")
 
     if args.cpu_worker:
-        cpu_worker(args.n, args.seed, args.load, args.iters, args.variant, args.out)
+        cpu_worker(args.n, args.seed, args.load, args.iters, args.variant, args.out,
+                   args.field, args.fftw)
         return
 
     world = env_int("WORLD_SIZE", 1)

@@ -9,7 +9,6 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 ULP = np.finfo(np.float64).eps
-REFERENCE = "/root/reference"
 
 
 def pytest_configure(config):

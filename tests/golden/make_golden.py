@@ -60,7 +60,9 @@ def checksum_weights(shape, s, seed=20240611):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference",
+                    default=os.environ.get("JANUS_REFERENCE", "/root/reference"),
+                    help="reference checkout (default $JANUS_REFERENCE)")
     args = ap.parse_args(argv)
     files = sorted(glob.glob(os.path.join(args.reference, "tests", "data",
                                           "*_green_operator_*.npz")))
