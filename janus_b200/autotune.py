@@ -76,6 +76,36 @@ def _key(green_op, nload):
                                    type(green_op).__name__, int(nload))
 
 
+def timing_local(green_op):
+    """A one-phase local operator with (C - C0) = 0 on the Green operator's
+    grid and precision: the pass times of a solver step do not depend on the
+    material, so the tuner can time the Green operator alone with it."""
+    from .operators import LocalPhaseOperator
+    grid = tuple(green_op.ishape[:-1])
+    return LocalPhaseOperator(len(grid), grid, np.zeros(grid, dtype=np.uint8), [0.0], [0.0],
+                              dtype=green_op.dtype)
+
+
+def _load_cache(path):
+    if os.path.exists(path):
+        try:
+            with open(path) as f:
+                return json.load(f)
+        except (OSError, ValueError):
+            pass
+    return {}
+
+
+def apply_cached(green_op, nload=1):
+    """Set the cached schedule of (green_op, nload) if the cache has one
+    (FFTW_MEASURE / FFTW_WISDOM_ONLY planning); True when set."""
+    entry = _load_cache(_cache_path()).get(_key(green_op, nload))
+    if entry is None:
+        return False
+    set_tuning(green_op, entry["tuning"])
+    return True
+
+
 def _time_passes(solver, eps, res, steps, warmup):
     for _ in range(warmup):
         solver.step(eps, res)
@@ -86,23 +116,20 @@ def _time_passes(solver, eps, res, steps, warmup):
     return {k: v / max(n, 1) for k, v in ms.items()}
 
 
-def tune(green_op, local_op, nload=1, steps=5, warmup=2, use_cache=True):
+def tune(green_op, local_op=None, nload=1, steps=5, warmup=2, use_cache=True):
     """Time the candidates on a solver step of (green_op, local_op, nload),
     set the fastest schedules on green_op and return
-    {"tuning": [6 values], "plain_ms": ..., "green_ms": ..., "cached": bool}."""
+    {"tuning": [6 values], "plain_ms": ..., "green_ms": ..., "cached": bool}.
+    Without local_op the passes are timed with a zero-contrast one."""
     path = _cache_path()
     key = _key(green_op, nload)
-    cache = {}
-    if use_cache and os.path.exists(path):
-        try:
-            with open(path) as f:
-                cache = json.load(f)
-        except (OSError, ValueError):
-            cache = {}
+    cache = _load_cache(path) if use_cache else {}
     if use_cache and key in cache:
         set_tuning(green_op, cache[key]["tuning"])
         return dict(cache[key], cached=True)
     dim = len(green_op.ishape) - 1
+    if local_op is None:
+        local_op = timing_local(green_op)
     solver = BasicScheme(green_op, local_op, nload)
     s = green_op.ishape[-1]
     E = np.eye(s)[np.arange(nload) % s]
@@ -114,17 +141,27 @@ def tune(green_op, local_op, nload=1, steps=5, warmup=2, use_cache=True):
     plain_c, green_c = candidates(dim, green_op.dtype)
     base = get_tuning(green_op)[:6]
     best_plain, best_green = (base[0:3], float("inf")), (base[3:6] + [0], float("inf"))
+    def timed(values):
+        """Pass times with the schedule `values`; None where a candidate
+        does not fit this grid (the native call rejects its tile)."""
+        try:
+            set_tuning(green_op, values)
+            return _time_passes(solver, eps, res, steps, warmup)
+        except ValueError:
+            return None
     # plain passes (3D): vary the plain schedule, Green schedule fixed
     for c in plain_c:
-        set_tuning(green_op, list(c) + base[3:6])
-        t = _time_passes(solver, eps, res, steps, warmup)
+        t = timed(list(c) + base[3:6])
+        if t is None:
+            continue
         ms = sum(t.get(p, 0.0) for p in _PLAIN_PASSES)
         if ms < best_plain[1]:
             best_plain = (list(c), ms)
     for mode in (1, 2):   # table, on the fly
         for c in green_c:
-            set_tuning(green_op, best_plain[0] + list(c) + [mode])
-            t = _time_passes(solver, eps, res, steps, warmup)
+            t = timed(best_plain[0] + list(c) + [mode])
+            if t is None:
+                continue
             ms = t.get(_GREEN_PASS, float("inf"))
             if ms < best_green[1]:
                 best_green = (list(c) + [mode], ms)

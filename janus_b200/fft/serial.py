@@ -58,6 +58,8 @@ class _RealFFT:
         L = _lib.lib()
         _lib.check(L.jb_fft_create(self._dim, _lib.i64_array(n), A.jb_dtype(self._dtype),
                                    int(flags), ctypes.byref(self._handle)))
+        # planning rigour, read by the Green operators built on this transform
+        self._flags = int(flags)
 
     def __del__(self):
         h = getattr(self, "_handle", None)

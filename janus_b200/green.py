@@ -15,7 +15,9 @@ finite-difference (Willot 2015) discretisations, 2D and 3D:
 
 ``transform`` may be None: unlike the reference (whose apply needs an FFT
 object), the GPU operator owns its transform plan, so apply works either
-way; a given transform must have ``global_ishape == n`` (green.pyx:115-118).
+way; a given transform must have ``global_ishape == n`` (green.pyx:115-118),
+and its planner flags choose how the column passes are scheduled on first
+use (see ``janus_b200.fft``).
 """
 from __future__ import annotations
 
@@ -88,6 +90,11 @@ class _DiscreteGreenOperator:
         self._h = h
         self._transform = transform
         self.init_shapes(*shape, green.isize, green.osize)
+        # schedule of the column passes, chosen on first use per batch size
+        # by the transform's planning rigour (janus_b200.fft); FFTW_MEASURE
+        # when no transform is given, as the reference's create_real default
+        self._planning = int(getattr(transform, "_flags", 0)) if transform is not None else 0
+        self._planned = set()
         self._handle = ctypes.c_void_p()
         mat = green.mat
         _lib.check(_lib.lib().jb_green_create(
@@ -176,7 +183,24 @@ class _DiscreteGreenOperator:
             ctypes.c_void_p(A.stream_handle())))
         return eta
 
+    def _plan(self, nload):
+        """FFTW_ESTIMATE: the built-in schedule rule; FFTW_MEASURE and
+        FFTW_WISDOM_ONLY: the autotuner's cached schedule if any;
+        FFTW_PATIENT / FFTW_EXHAUSTIVE: run the autotuner once (cached)."""
+        if nload in self._planned:
+            return
+        self._planned.add(nload)
+        from .fft.serial import FFTW_ESTIMATE, FFTW_EXHAUSTIVE, FFTW_PATIENT
+        if self._planning & FFTW_ESTIMATE:
+            return
+        from . import autotune
+        if self._planning & (FFTW_PATIENT | FFTW_EXHAUSTIVE):
+            autotune.tune(self, None, nload=nload)
+        else:
+            autotune.apply_cached(self, nload)
+
     def _apply_device(self, x, y):
+        self._plan(1)
         _lib.check(_lib.lib().jb_green_apply(self._handle, ctypes.c_void_p(x.data_ptr()),
                                              ctypes.c_void_p(y.data_ptr()), 1,
                                              ctypes.c_void_p(A.stream_handle())))
@@ -188,6 +212,7 @@ class _DiscreteGreenOperator:
         xd = A.to_device(x, self._dtype)
         if y is None:
             y = xd.new_empty(xd.shape)
+        self._plan(int(xd.shape[0]))
         _lib.check(_lib.lib().jb_green_apply(self._handle, ctypes.c_void_p(xd.data_ptr()),
                                              ctypes.c_void_p(y.data_ptr()), int(xd.shape[0]),
                                              ctypes.c_void_p(A.stream_handle())))
