@@ -145,9 +145,12 @@ int jb_green_apply(jb_green *green, const void *x, void *y, int64_t batch,
  * until exit.  Limit: the half spectrum n0*(n1)*(n_last/2+1)*s*16 bytes must
  * fit in 31 MiB (FP64 2D up to about 1024 x 1024, 3D up to about 80^3) and
  * no axis may exceed 4096; larger grids get JB_EINVAL with the size in the
- * message.  The first call on a device (with that device current) looks up
- * the array's address, so make it before any stream capture.  Calls share
- * the array: calls that overlap on the GPU race. */
+ * message.  x and y must be memory of the current device and `stream` one
+ * of its streams (else JB_EINVAL).  The first call on a device (with that
+ * device current) looks up the array's address and caches it (the cache
+ * does not survive cudaDeviceReset), so make it before any stream capture.
+ * Each call fills the twiddles and tables with a kernel on `stream` (no host
+ * copies).  Calls share the array: calls that overlap on the GPU race. */
 int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
                            double nu, int variant, const double *x, double *y,
                            void *stream);

@@ -1593,8 +1593,11 @@ extern "C" int jb_gmres_run(jb_gmres* S, const double* E, void* eps, int init, i
 //
 // Set-up: the first call on a device, with that device current, looks up the
 // array's device address (cudaGetSymbolAddress) and caches it per device, so
-// make the first call on each device before any stream capture.  The array
-// keeps the last call's contents; nothing in it needs to start at zero (every
+// make the first call on each device before any stream capture.  The cache
+// does not survive a device reset (cudaDeviceReset) in the same process.
+// Every call fills the twiddles and the k / weight tables on the device with
+// one small kernel (no host copies), then runs the passes.  The array keeps
+// the last call's contents; nothing in it needs to start at zero (every
 // region is written before it is read within a call).  Calls share the
 // array, so two calls that overlap on the GPU (different streams, or
 // different host threads without ordering) race.
@@ -1634,6 +1637,78 @@ int noalloc_scratch(void** out) {
   return JB_OK;
 }
 
+// per-axis data of one allocation-free call, passed by value
+struct NoallocAxes {
+  int dim, variant;
+  int n[3];
+  double s[3];  // 2 pi / (h n_d), as the handle-based operator computes it
+  double h;
+};
+
+// twiddles exp(-2 pi i t / n) and the per-axis k (truncated) or k-, k+, w-,
+// w+ (filtered) tables of green.pyx:434-445 / 609-670, into the static array
+__global__ void noalloc_fill_kernel(NoallocAxes a) {
+  for (int d = 0; d < a.dim; ++d) {
+    const int n = a.n[d];
+    const double sd = a.s[d];
+    double2* tw =
+        reinterpret_cast<double2*>(g_noalloc_scratch + kNoAllocTwOff + d * kNoAllocTwBytes);
+    double* tab[4];
+    for (int i = 0; i < 4; ++i)
+      tab[i] = reinterpret_cast<double*>(g_noalloc_scratch + kNoAllocTabOff +
+                                         (size_t)(d * 4 + i) * kNoAllocTabBytes);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+      double sn, cs;
+      sincospi(2.0 * (double)t / (double)n, &sn, &cs);
+      tw[t] = make_double2(cs, -sn);
+      if (a.variant == JB_TRUNCATED) {
+        tab[0][t] = 2 * t > n ? sd * (double)(t - n) : sd * (double)t;
+      } else {
+        double k = sd * (double)(t - n);
+        double w = cos(0.25 * a.h * k);
+        tab[0][t] = k;
+        tab[2][t] = w * w;
+        k = sd * (double)t;
+        w = cos(0.25 * a.h * k);
+        tab[1][t] = k;
+        tab[3][t] = w * w;
+      }
+    }
+  }
+}
+
+// x / y must be memory of the current device, and the stream one of its
+// streams: the kernels address this device's static array
+int noalloc_check_device(const void* x, const void* y, cudaStream_t st) {
+  int dev = -1;
+  JB_CUDA(cudaGetDevice(&dev));
+  for (const void* p : {x, y}) {
+    cudaPointerAttributes at{};
+    const cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(JB_EINVAL, "jb_green_apply_noalloc: x and y must be device memory");
+    }
+    if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) ||
+        at.device != dev)
+      return fail(JB_EINVAL, "jb_green_apply_noalloc: x and y must be memory of the current "
+                             "device (" + std::to_string(dev) + ")");
+  }
+  if (st) {
+    int sdev = -1;
+    const cudaError_t e = cudaStreamGetDevice(st, &sdev);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(JB_EINVAL, "jb_green_apply_noalloc: invalid stream");
+    }
+    if (sdev != dev)
+      return fail(JB_EINVAL, "jb_green_apply_noalloc: the stream belongs to device " +
+                                 std::to_string(sdev) + ", not the current device " +
+                                 std::to_string(dev));
+  }
+  return JB_OK;
+}
+
 }  // namespace
 
 extern "C" int jb_green_apply_noalloc(int dim, const int64_t* shape, double h, double g,
@@ -1656,10 +1731,11 @@ extern "C" int jb_green_apply_noalloc(int dim, const int64_t* shape, double h, d
                                " bytes of spectral scratch; the static scratch holds " +
                                std::to_string(kNoAllocBytes - kNoAllocSpecOff) +
                                " (FP64: 2D up to about 1024 x 1024, 3D up to about 80^3)");
+  cudaStream_t st = as_stream(stream);
+  JB_TRY(noalloc_check_device(x, y, st));
   void* base = nullptr;
   JB_TRY(noalloc_scratch(&base));
   unsigned char* b8 = static_cast<unsigned char*>(base);
-  cudaStream_t st = as_stream(stream);
 
   // a stack-held operator description whose device pointers all point into
   // the static array (no handle, no allocation)
@@ -1674,48 +1750,28 @@ extern "C" int jb_green_apply_noalloc(int dim, const int64_t* shape, double h, d
   G.gt.variant = variant;
   G.gt.inv2g = 0.5 / g;
   G.gt.c1 = 1.0 / (1.0 - nu);
-  const long double two_pi = 6.283185307179586476925286766559005768L;
-  std::vector<double> tw, tab[4];
+  NoallocAxes ax{};
+  ax.dim = dim;
+  ax.variant = variant;
+  ax.h = h;
+  int nmax = 1;
   for (int d = 0; d < dim; ++d) {
     const int64_t n = shape[d];
     G.n[d] = n;
     G.s[d] = 2. * M_PI / (h * (double)n);
     factorize((int)n, G.ax[d].plan);
-    tw.resize(2 * (size_t)n);
-    for (int64_t t = 0; t < n; ++t) {
-      long double a = two_pi * (long double)t / (long double)n;
-      tw[2 * t] = (double)cosl(a);
-      tw[2 * t + 1] = (double)-sinl(a);
-    }
     G.ax[d].tw = b8 + kNoAllocTwOff + d * kNoAllocTwBytes;
-    JB_CUDA(cudaMemcpyAsync(G.ax[d].tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice, st));
-    const double sd = G.s[d];
-    for (auto& v : tab) v.assign(n, 0.0);
-    for (int64_t b = 0; b < n; ++b) {
-      if (variant == JB_TRUNCATED) {
-        tab[0][b] = 2 * b > n ? sd * (b - n) : sd * b;
-      } else {
-        double k = sd * (b - n);
-        double w = cos(0.25 * h * k);
-        w *= w;
-        tab[0][b] = k;
-        tab[2][b] = w;
-        k = sd * b;
-        w = cos(0.25 * h * k);
-        w *= w;
-        tab[1][b] = k;
-        tab[3][b] = w;
-      }
-    }
+    ax.n[d] = (int)n;
+    ax.s[d] = G.s[d];
+    nmax = std::max(nmax, (int)n);
     void** slots[4] = {variant == JB_TRUNCATED ? &G.gt.kt[d] : &G.gt.kn[d], &G.gt.kp[d],
                        &G.gt.wn[d], &G.gt.wp[d]};
     const int ntab = variant == JB_TRUNCATED ? 1 : 4;
-    for (int i = 0; i < ntab; ++i) {
-      void* dst = b8 + kNoAllocTabOff + (size_t)(d * 4 + i) * kNoAllocTabBytes;
-      JB_CUDA(cudaMemcpyAsync(dst, tab[i].data(), n * 8, cudaMemcpyHostToDevice, st));
-      *slots[i] = dst;
-    }
+    for (int i = 0; i < ntab; ++i)
+      *slots[i] = b8 + kNoAllocTabOff + (size_t)(d * 4 + i) * kNoAllocTabBytes;
   }
+  noalloc_fill_kernel<<<(nmax + 255) / 256, 256, 0, st>>>(ax);
+  JB_TRY(launch_status(cudaGetLastError(), "noalloc_fill"));
   const int r = green_passes(&G, x, y, 1, b8 + kNoAllocSpecOff, nullptr, nullptr, nullptr, st);
   for (int d = 0; d < 3; ++d) G.ax[d].tw = nullptr;  // not owned
   return r;

@@ -62,3 +62,36 @@ def test_noalloc_matches_green_apply_on_consecutive_calls():
     big = torch.empty(1, dtype=torch.float64, device="cuda")
     assert _noalloc(big, (128, 128, 128), 1.0, 1.0, 0.3, 0, big) == _lib.JB_EINVAL
     assert b"static scratch" in _lib.lib().jb_last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_warm_call_leaves_free_device_memory_unchanged():
+    """The point of the entry point: a warm call allocates nothing, so the
+    device's free memory is the same before and after it."""
+    rng = np.random.default_rng(7)
+    shape = (48, 40, 36)
+    x = torch.from_numpy(rng.normal(size=shape + (6,))).cuda()
+    y = torch.empty_like(x)
+    assert _noalloc(x, shape, 1.0, 0.75, 0.3, _lib.JB_FILTERED, y) == 0   # warm
+    torch.cuda.synchronize()
+    first = y.clone()
+    free0, _ = torch.cuda.mem_get_info()
+    assert _noalloc(x, shape, 1.0, 0.75, 0.3, _lib.JB_FILTERED, y) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.equal(y, first)
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_host_pointers():
+    x = np.zeros((16, 16, 3))
+    dims = (ctypes.c_int64 * 2)(16, 16)
+    fn = _lib.lib().jb_green_apply_noalloc
+    fn.argtypes = [ctypes.c_int, P64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                   ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    r = fn(2, dims, 1.0, 1.0, 0.3, 0, ctypes.c_void_p(x.ctypes.data),
+           ctypes.c_void_p(x.ctypes.data), None)
+    assert r == _lib.JB_EINVAL
+    assert b"device" in _lib.lib().jb_last_error()
