@@ -9,6 +9,9 @@ reproducible):
 * ``random_spheres``: non-overlapping spheres by random sequential addition
   under periodic distance, up to a volume fraction;
 * ``ellipses``: 2D random elliptical inclusions with periodic wrap;
+* ``ellipsoid``: one centred ellipse / ellipsoid on a cartesian grid of
+  given physical size (the generator of notebooks/gen_ellipsoid.py:12-38,
+  without its HDF5 output: h5py is not part of this build);
 * ``voronoi``: periodic nearest-site partition with a random phase per cell;
 * ``gaussian_field``: a stationary Gaussian random field with squared-
   exponential correlation, made by spectral filtering of white noise.
@@ -33,6 +36,28 @@ def square_inclusion(n, side=None, centered=True, a=0.5):
         imax = int(np.ceil(n * a - 0.5))
         phase[:imax, :imax] = 1
     return phase
+
+
+def ellipsoid(radii, size, shape):
+    """int8 phase map of a 2D ellipse or 3D ellipsoid centred in a grid.
+
+    ``radii`` (2 or 3 floats) and ``size`` (the grid's side lengths) are in
+    the same units of length; ``shape`` is the number of cells per side.
+    A cell is 1 when its centre lies inside or on the ellipsoid, else 0
+    (notebooks/gen_ellipsoid.py:12-38).  Cell centres along an axis of
+    length L and n cells sit at -L(n-1)/(2n) ... L(n-1)/(2n), n evenly
+    spaced points."""
+    radii, size, shape = tuple(radii), tuple(size), tuple(int(n) for n in shape)
+    if not (len(radii) == len(size) == len(shape)) or len(shape) not in (2, 3):
+        raise ValueError("radii, size and shape must all have length 2 or 3")
+    acc = np.zeros(shape)
+    for d, (r, L, n) in enumerate(zip(radii, size, shape)):
+        h = 0.5 * L * (n - 1) / n
+        c = np.linspace(-h, h, num=n) / r
+        view = [1] * len(shape)
+        view[d] = n
+        acc = acc + (c * c).reshape(view)
+    return (acc <= 1).astype(np.int8)
 
 
 def _periodic_delta(d, n):
