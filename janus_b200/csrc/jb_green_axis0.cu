@@ -10,10 +10,12 @@
 //   X[k1 + NL k2] = sum_j w4^(j k2) w_n0^(j k1) sum_m x[j + 4 m] w_NL^(m k1).
 // Phase 1: the lanes of a (load case, column, j) slice load its NL values of
 //          the column straight from global memory into registers and compute
-//          the NL-point transform over m in registers (one lane for NL <= 16;
-//          for NL = 32 a lane pair, each lane a 16-point transform of half
-//          the rows, then one radix-2 step exchanged by shuffles), then store
-//          the NL results in shared memory.
+//          the NL-point transform over m in registers: one lane for NL <= 16;
+//          for NL = 16 S, S lanes (m = a + S b), each a 16-point transform
+//          of its rows, a twiddle, then an S-point transform across the
+//          lanes by shuffles (S = 2: one radix-2 step with compile-time
+//          twiddles; S = 4..16: radix-2 steps and a bit-reversal exchange);
+//          then the NL results go to shared memory.
 // Phase 2: one thread per (load case, k1, group of 6 columns: one 3D
 //          coefficient or two 2D ones) reads its 4 x 6 values, applies the
 //          twiddles w_n0^(j k1) and the 4-point transform over j, contracts
@@ -22,10 +24,9 @@
 // Phase 3: the phase-1 lanes read their values, transform back and store
 //          the column to global memory.
 // Each spectral value therefore crosses shared memory twice each way and is
-// read and written once in HBM; the twiddles of the in-lane transforms are
-// compile-time constants.  A tile holds two load cases of the same
-// coefficients, so the two lanes of a phase-2 pair read the same table
-// entries in one broadcast.  The next tile's rows are prefetched into L2
+// read and written once in HBM.  Up to n0 = 256 a tile holds two load cases
+// of the same coefficients, so the two lanes of a phase-2 pair read the same
+// table entries in one broadcast.  The next tile's rows are prefetched into L2
 // while the current tile is transformed.  There are no waits besides the
 // block barriers.  The result is unnormalised (the c2r pass scales by 1/N,
 // as janus/fft/serial/_serial_fft.pyx:121-150 does).
@@ -76,18 +77,17 @@ template <typename C> __device__ __forceinline__ C shfl_xor1(C v) {
   return mkc(__shfl_xor_sync(0xffffffffu, v.x, 1), __shfl_xor_sync(0xffffffffu, v.y, 1));
 }
 
-// lanes per column slice and values a lane holds: NL = 32 is split over a
-// lane pair (16 values each, one radix-2 exchange by shuffles); NL <= 16 is
-// held by one lane
+// lanes per column slice and values a lane holds: NL <= 16 is held by one
+// lane; NL = 16 S (S = 2, 4, 8, 16) is split over S consecutive lanes of a
+// warp, 16 values each, m = a + S b for lane a
 template <int NL> struct LaneSplit {
-  static constexpr int SPL = NL == 32 ? 2 : 1;
+  static constexpr int SPL = NL <= 16 ? 1 : NL / 16;
   static constexpr int V = NL / SPL;
 };
 
-// row (relative to j) of value i of lane a: m = a + 2 i for the pair split,
-// m = i otherwise (n = j + 4 m)
+// row (relative to j) of value i of lane a (n = j + 4 m)
 template <int NL> __device__ __forceinline__ int lane_row(int i, int a) {
-  return NL == 32 ? 4 * a + 8 * i : 4 * i;
+  return 4 * (a + LaneSplit<NL>::SPL * i);
 }
 
 template <int E, typename C> struct PairLoop {
@@ -113,24 +113,76 @@ template <typename C> struct PairLoop<16, C> {
   __device__ __forceinline__ static void inv(C*, bool) {}
 };
 
+template <int S> __device__ __forceinline__ int bit_reverse(int x) {
+  int r = 0;
+#pragma unroll
+  for (int m = 1; m < S; m <<= 1) {
+    r = (r << 1) | (x & 1);
+    x >>= 1;
+  }
+  return r;
+}
+
+// S-point DFT across the S lanes of a slice (S = 4, 8, 16) for each of the
+// 16 values: lane a holds V_a[e]; on return lane d holds
+// sum_a w_S^(DIR a d) V_a[e].  Radix-2 decimation in frequency over the lane
+// index (the lower lane of a pair keeps u + o, the upper (o - u) w_2h^q,
+// q = a mod h), then a bit-reversal permutation of the lanes.  tw: the
+// axis table exp(-2 pi i t / n0), n0 = 64 S.
+template <int S, int DIR, typename C>
+__device__ __forceinline__ void cross_lane_dft(C* v, int a, const C* tw) {
+  constexpr int N0 = 64 * S;
+#pragma unroll
+  for (int h = S / 2; h >= 1; h >>= 1) {
+    const bool upper = (a & h) != 0;
+    C w = tw[(a % h) * (N0 / (2 * h))];
+    if (DIR > 0) w = cconj(w);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const C u = v[e];
+      const C o = mkc(__shfl_xor_sync(0xffffffffu, u.x, h), __shfl_xor_sync(0xffffffffu, u.y, h));
+      v[e] = upper ? cmul(csub(o, u), w) : cadd(u, o);
+    }
+  }
+  const int src = ((threadIdx.x & 31) & ~(S - 1)) | bit_reverse<S>(a);
+#pragma unroll
+  for (int e = 0; e < 16; ++e)
+    v[e] = mkc(__shfl_sync(0xffffffffu, v[e].x, src), __shfl_sync(0xffffffffu, v[e].y, src));
+}
+
 // forward transform over m of a column slice: on entry v[i] holds row
 // j + 4 m(i, a); on return v[i] = Y[k1] at k1 = i + V a
-template <int NL, typename C> __device__ __forceinline__ void lane_fwd(C* v, bool odd) {
-  if constexpr (NL == 32) {
-    Dft<16, -1, C>::run(v);
-    PairLoop<0, C>::fwd(v, odd);
-  } else {
+template <int NL, typename C>
+__device__ __forceinline__ void lane_fwd(C* v, int a, const C* tw) {
+  constexpr int S = LaneSplit<NL>::SPL;
+  if constexpr (S == 1) {
     Dft<NL, -1, C>::run(v);
+  } else if constexpr (S == 2) {
+    Dft<16, -1, C>::run(v);
+    PairLoop<0, C>::fwd(v, a != 0);
+  } else {
+    Dft<16, -1, C>::run(v);
+    // V_a[e] = w_NL^(a e) U_a[e], w_NL = w_n0^4
+#pragma unroll
+    for (int e = 1; e < 16; ++e) v[e] = cmul(v[e], tw[4 * a * e]);
+    cross_lane_dft<S, -1>(v, a, tw);
   }
 }
 
 // inverse: v[i] = V[k1] at k1 = i + V a -> v[i] = x at row j + 4 m(i, a)
-template <int NL, typename C> __device__ __forceinline__ void lane_inv(C* v, bool odd) {
-  if constexpr (NL == 32) {
-    PairLoop<0, C>::inv(v, odd);
+template <int NL, typename C>
+__device__ __forceinline__ void lane_inv(C* v, int a, const C* tw) {
+  constexpr int S = LaneSplit<NL>::SPL;
+  if constexpr (S == 1) {
+    Dft<NL, +1, C>::run(v);
+  } else if constexpr (S == 2) {
+    PairLoop<0, C>::inv(v, a != 0);
     Dft<16, +1, C>::run(v);
   } else {
-    Dft<NL, +1, C>::run(v);
+    cross_lane_dft<S, +1>(v, a, tw);
+#pragma unroll
+    for (int e = 1; e < 16; ++e) v[e] = cmulc(v[e], tw[4 * a * e]);
+    Dft<16, +1, C>::run(v);
   }
 }
 
@@ -138,22 +190,22 @@ template <int NL, typename C> __device__ __forceinline__ void lane_inv(C* v, boo
 // coefficient; 2D: C = 3, two coefficients)
 template <typename T, int DIM, int NL> struct R4Tile {
   static constexpr int C = DIM == 3 ? 6 : 3;
-  static constexpr int LT = 2;                    // load cases per tile
-  static constexpr int NG = 128 / (LT * NL);      // 6-column groups per tile
+  static constexpr int LT = NL <= 64 ? 2 : 1;     // load cases per tile
+  static constexpr int NG = NL <= 64 ? 128 / (LT * NL) : 1;  // 6-column groups per tile
   static constexpr int WC = 6 * NG;               // columns per tile
   static constexpr int SPL = LaneSplit<NL>::SPL;
   static constexpr int P1 = LT * WC * 4 * SPL;    // phase-1/3 threads
-  static constexpr int P2 = 128;                  // phase-2 threads
+  static constexpr int P2 = LT * NL * NG;         // phase-2 threads
   static constexpr int THREADS = P1 > P2 ? P1 : P2;
   static constexpr int P = 4 * WC + 1;            // k1 stride (odd)
   // shared-memory phases: 8 lanes of 16 bytes (FP64), 16 of 8 bytes (FP32)
   static constexpr int LMOD = sizeof(T) == 8 ? 8 : 16;
-  // values k1 >= 16 of a pair-split slice sit LMOD/2 further on, so that the
-  // two lanes of a pair write disjoint banks
-  static constexpr int HI = SPL == 2 ? LMOD / 2 : 0;
+  // block d of 16 values (lane d of a split slice) sits d OSTEP further on,
+  // so that the lanes of a slice write disjoint banks
+  static constexpr int OSTEP = SPL == 1 ? 0 : (SPL >= LMOD ? 1 : LMOD / SPL);
   // load-case stride: past the last value, and LMOD/2 mod LMOD, so that the
   // two load cases of a phase-2 lane pair fall in disjoint banks
-  static constexpr int LS0 = NL * P + HI;
+  static constexpr int LS0 = NL * P + SPL * OSTEP;
   static constexpr int LS = LS0 + ((LMOD / 2 - LS0 % LMOD) + LMOD) % LMOD;
   static constexpr size_t SMEM = (size_t)LT * LS * sizeof(cx<T>);
   // resident CTAs asked of the register allocator
@@ -162,7 +214,7 @@ template <typename T, int DIM, int NL> struct R4Tile {
 
 // offset of value k1 in a (load case, j, column) slice
 template <typename K> __device__ __forceinline__ int k1_off(int k1) {
-  return k1 * K::P + (K::HI != 0 && k1 >= 16 ? K::HI : 0);
+  return k1 * K::P + (k1 >> 4) * K::OSTEP;
 }
 
 template <typename T> struct Axis0Args {
@@ -238,7 +290,7 @@ __global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL
   const int tid = threadIdx.x;
   // phase-1/3 lane: half a of a pair (pair split), column c, load case l1, j1
   const bool p1 = tid < K::P1;
-  const int a1 = K::SPL == 2 ? (tid & 1) : 0;
+  const int a1 = tid % K::SPL;
   const int s1 = tid / K::SPL;
   const int c = s1 % K::WC;
   const int l1 = (s1 / K::WC) % K::LT;
@@ -285,7 +337,7 @@ __global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL
 #pragma unroll
       for (int i = 0; i < NV; ++i)
         v[i] = ok1 ? src[(int64_t)lane_row<NL>(i, a1) * pitch] : mkc(T(0), T(0));
-      lane_fwd<NL>(v, a1 != 0);
+      lane_fwd<NL>(v, a1, a.tw);
     }
     __syncthreads();  // the previous tile's phase 3 has read S
     if (p1) {
@@ -345,7 +397,7 @@ __global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL
       const C* s = S + l1 * K::LS + j1 * K::WC + c;
 #pragma unroll
       for (int i = 0; i < NV; ++i) v[i] = s[k1_off<K>(i + NV * a1)];
-      lane_inv<NL>(v, a1 != 0);
+      lane_inv<NL>(v, a1, a.tw);
       if (ok1) {
         int64_t pitch3;
         asm volatile("mov.b64 %0, %1;" : "=l"(pitch3) : "l"(a.pitch));
@@ -391,16 +443,21 @@ cudaError_t axis0_go(const Axis0Args<T>& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <typename T, int DIM, bool TAB>
+cudaError_t axis0_n(const Axis0Args<T>& a, int n0, cudaStream_t st) {
+  switch (n0) {
+    case 32: return axis0_go<T, DIM, 8, TAB>(a, st);
+    case 64: return axis0_go<T, DIM, 16, TAB>(a, st);
+    case 128: return axis0_go<T, DIM, 32, TAB>(a, st);
+    case 256: return axis0_go<T, DIM, 64, TAB>(a, st);
+    case 512: return axis0_go<T, DIM, 128, TAB>(a, st);
+    default: return axis0_go<T, DIM, 256, TAB>(a, st);
+  }
+}
+
 template <typename T, bool TAB>
 cudaError_t axis0_dim(const Axis0Args<T>& a, int n0, int dim, cudaStream_t st) {
-  if (dim == 3) {
-    if (n0 == 128) return axis0_go<T, 3, 32, TAB>(a, st);
-    if (n0 == 64) return axis0_go<T, 3, 16, TAB>(a, st);
-    return axis0_go<T, 3, 8, TAB>(a, st);
-  }
-  if (n0 == 128) return axis0_go<T, 2, 32, TAB>(a, st);
-  if (n0 == 64) return axis0_go<T, 2, 16, TAB>(a, st);
-  return axis0_go<T, 2, 8, TAB>(a, st);
+  return dim == 3 ? axis0_n<T, 3, TAB>(a, n0, st) : axis0_n<T, 2, TAB>(a, n0, st);
 }
 
 template <typename T>
@@ -447,7 +504,8 @@ cudaError_t axis0_t(const AxisData& ax0, int64_t L, int64_t inner, int64_t pitch
 }  // namespace
 
 bool green_axis0_r4_supported(int n0, int C, int dim) {
-  return (n0 == 32 || n0 == 64 || n0 == 128) && ((dim == 3 && C == 6) || (dim == 2 && C == 3));
+  return (n0 == 32 || n0 == 64 || n0 == 128 || n0 == 256 || n0 == 512 || n0 == 1024) &&
+         ((dim == 3 && C == 6) || (dim == 2 && C == 3));
 }
 
 cudaError_t launch_green_axis0_r4(int dtype, const AxisData& ax0, int64_t L, int64_t inner,

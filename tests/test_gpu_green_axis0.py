@@ -1,5 +1,5 @@
 """The axis-0 Green pass whose middle radix-4 stage and contraction run in
-registers (n0 = 32, 64, 128), against the oracle and against the
+registers (n0 = 32 ... 1024), against the oracle and against the
 shared-memory column kernel, for the three discretisations of
 janus/green.pyx (truncated 393-580, filtered 583-973 through the generic
 c_apply 185-216 / 356-390, finite differences 976-1036).
@@ -19,8 +19,10 @@ from oracle import janus_oracle as O
 MU = 0.75
 NU = 0.3
 FACTORY = {"truncated": truncated, "filtered": filtered, "willot": willot2015}
-# n0 in {128, 64, 32}; coefficient counts 36, 25, 36 (3D) and 10, 4, 17 (2D)
-SHAPES = [(128, 6, 10), (64, 5, 8), (32, 9, 6), (128, 18), (64, 7), (32, 33)]
+# n0 from 32 to 1024 (one lane per column slice up to 64, split over 2 to 16
+# lanes above); ragged coefficient counts in the last tile
+SHAPES = [(128, 6, 10), (64, 5, 8), (32, 9, 6), (256, 3, 6), (512, 2, 4), (1024, 1, 6),
+          (128, 18), (64, 7), (32, 33), (256, 10), (512, 6), (1024, 14)]
 # register radix-4 Green pass (compile-time value 3), the contraction by the
 # built-in rule
 R4 = [0, 0, 1, 0, 0, 3, 0]
@@ -76,7 +78,7 @@ def test_r4_table_and_on_the_fly(mode, shape):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant", ["truncated", "filtered"])
-@pytest.mark.parametrize("shape", [(128, 10, 12), (64, 33)])
+@pytest.mark.parametrize("shape", [(128, 10, 12), (64, 33), (256, 4, 6), (1024, 10)])
 def test_r4_fp32(variant, shape):
     """FP32 fields through the same pass: within FP32 rounding of the FP64 oracle."""
     rng = np.random.default_rng(9)
