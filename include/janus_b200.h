@@ -322,11 +322,12 @@ int jb_mixed_run(jb_mixed *solver, const double *E, void *eps, int init,
 /* Batched mixed-precision solves (no reference counterpart): `count`
  * problems, each a jb_mixed solver of its own grid (sizes may differ) and
  * load cases.  jb_batch_run evaluates every problem's first FP64 residual,
- * then launches one CUDA graph per outer step that holds, for every problem
- * still iterating, the FP32 correction sweeps and the next FP64 residual;
- * the problems run on `branches` parallel streams inside the graph (largest
- * first onto the least loaded).  The graph is captured again only when a
- * problem leaves the iteration (converged or at max_outer).  Arrays are
+ * then runs the outer steps (the FP32 correction sweeps and the next FP64
+ * residual of every problem still iterating) in one CUDA graph launch (see
+ * jb_batch_set_persistent; per-step form: one launch per outer step, the
+ * problems on `branches` parallel streams inside the graph, largest first
+ * onto the least loaded, captured again only when a problem leaves the
+ * iteration, converged or at max_outer).  Arrays are
  * concatenated in problem order: E host double[L_p][s_p]; eps device
  * pointers (FP64 fields [L_p][grid_p][s_p]); residuals host
  * double[max_outer][L_p] per problem (may be NULL); outer_out /
@@ -338,6 +339,15 @@ typedef struct jb_batch_s jb_batch;
 int jb_batch_create(int count, jb_mixed *const *problems, int branches,
                     jb_batch **out);
 int jb_batch_destroy(jb_batch *batch);
+/* on != 0 (the default): jb_batch_run makes ONE graph launch for the whole
+ * run: a while node whose body runs a decision kernel (each problem's
+ * residuals recorded and its load cases' outcomes updated on the device,
+ * problems retired as on the host) and, per problem, an if node holding its
+ * correction and FP64 residual; no host readback until the end.  on == 0:
+ * one graph launch per outer step with the decision on the host.  Results
+ * are bitwise the same.  Where conditional graph nodes are unavailable the
+ * run falls back to the per-step form. */
+int jb_batch_set_persistent(jb_batch *batch, int on);
 int jb_batch_run(jb_batch *batch, const double *E, void *const *eps, int init,
                  int max_outer, int inner, double tol, double *residuals,
                  int *outer_out, int *fp32_iters_out, double *mean_tau,

@@ -76,6 +76,7 @@ _SIGS = {
     "jb_batch_create": ([c_int, ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)],
                         c_int),
     "jb_batch_destroy": ([c_void_p], c_int),
+    "jb_batch_set_persistent": ([c_void_p, c_int], c_int),
     "jb_batch_run": ([c_void_p, P_double, ctypes.POINTER(c_void_p), c_int, c_int, c_int,
                       c_double, P_double, P_int, P_int, P_double, P_int, P_int, c_void_p],
                      c_int),

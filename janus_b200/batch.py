@@ -5,11 +5,14 @@ No counterpart in the reference, whose loop (square_basic.py:83-97) solves
 one cell at a time in FP64.  Each problem is a ``MixedScheme`` (FP32 bulk
 iterations, FP64 defect correction) over its own grid and load cases; the
 native ``jb_batch`` runtime evaluates every problem's first FP64 residual,
-then captures one outer step of all problems still iterating (FP32
-correction sweeps, then the next FP64 residual) into a CUDA graph whose
-branches run the problems concurrently, and launches that graph once per
-outer step.  The residuals of all problems come back in one copy per step;
-the graph is captured again only when a problem converges.
+then runs the whole iteration as ONE CUDA graph launch: a while node whose
+body is a decision kernel (residuals recorded, outcomes updated, converged
+or stopped problems retired, on the device) followed by one if node per
+problem holding its FP32 correction sweeps and next FP64 residual, so the
+problems run concurrently and the host reads nothing back until the end.
+``persistent=False`` keeps the per-step form (one graph launch per outer
+step, residuals read back each step, the graph captured again when a
+problem leaves); results are bitwise the same.
 """
 from __future__ import annotations
 
@@ -31,7 +34,7 @@ class BatchedMixedScheme:
     BiCGSTAB iterations (a lone MixedScheme sizes them adaptively); the
     results equal one-by-one solves with method "bicgstab_fixed" bitwise."""
 
-    def __init__(self, problems, inner=20, branches=8, method="basic"):
+    def __init__(self, problems, inner=20, branches=8, method="basic", persistent=True):
         if not problems:
             raise ValueError("a batch needs at least one problem")
         self.schemes = [MixedScheme(g, l, nload, inner, method=method)
@@ -42,6 +45,7 @@ class BatchedMixedScheme:
         self._handle = ctypes.c_void_p()
         _lib.check(_lib.lib().jb_batch_create(len(self.schemes), handles, int(branches),
                                               ctypes.byref(self._handle)))
+        _lib.check(_lib.lib().jb_batch_set_persistent(self._handle, int(bool(persistent))))
         self.graph_launches = 0
 
     def __del__(self):

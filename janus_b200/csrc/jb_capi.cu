@@ -2114,6 +2114,8 @@ struct jb_batch_s {
   DeviceBuf res_all;
   size_t nres = 0;
   cudaGraphExec_t exec = nullptr;
+  DeviceBuf dstate;                    // persistent run: decision state on the device
+  bool persistent = true;              // one graph launch per run (conditional nodes)
   std::vector<char> captured;          // active set of the instantiated graph
   std::vector<void*> captured_eps;     // the strain fields its kernels address
   int captured_inner = 0;
@@ -2126,6 +2128,12 @@ extern "C" int jb_batch_destroy(jb_batch* B) {
   for (cudaEvent_t e : B->events) cudaEventDestroy(e);
   if (B->res_all.p) cudaFree(B->res_all.p);
   delete B;
+  return JB_OK;
+}
+
+extern "C" int jb_batch_set_persistent(jb_batch* B, int on) {
+  if (!B) return fail(JB_EINVAL, "NULL argument");
+  B->persistent = on != 0;
   return JB_OK;
 }
 
@@ -2231,6 +2239,239 @@ int batch_capture(jb_batch* B, const std::vector<char>& active, void* const* eps
 
 }  // namespace
 
+namespace {
+
+// Device-side decision of the persistent batched run: the host loop's
+// per-step work (record each active problem's residuals, update each load
+// case's outcome, retire problems that converged, stopped or reached
+// max_outer) done by one block at the start of every iteration of the
+// graph's while node; it sets each problem's IF condition and the while
+// condition (any problem active).  Same rule as Outcome::update.
+struct BatchDecide {
+  int P, max_outer;
+  double tol, diverge;
+  const int* L;               // [P] load cases
+  const int* roff;            // [P] offset of a problem's load cases in res / best / ...
+  const int64_t* hoff;        // [P] offset of a problem's history (max_outer x L)
+  const double* res;          // [nres] latest residuals
+  double* hist;               // residual history
+  double* best;               // [nres]
+  double* last;               // [nres]
+  int* stopped;               // [nres]
+  int* active;                // [P]
+  int* outer;                 // [P] residual evaluations recorded + 1 while iterating
+  int* steps;                 // iterations of the while body so far (bound)
+  const cudaGraphConditionalHandle* ifh;  // [P]
+  cudaGraphConditionalHandle wh;
+};
+
+__global__ void batch_decide_kernel(BatchDecide a) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  // the while body runs at most max_outer + 1 times (every problem retires
+  // by then); past that, retire everything
+  const bool force = *a.steps > a.max_outer + 1;
+  for (int p = threadIdx.x; p < a.P; p += blockDim.x) {
+    int act = a.active[p];
+    if (act) {
+      const int L = a.L[p], o = a.outer[p];
+      bool done = true;
+      for (int l = 0; l < L; ++l) {
+        const int q = a.roff[p] + l;
+        const double r = a.res[q];
+        a.hist[a.hoff[p] + (int64_t)(o - 1) * L + l] = r;
+        bool fin;  // the load case no longer holds the problem back
+        if (a.stopped[q]) {
+          fin = true;
+        } else {
+          a.last[q] = r;
+          if (!isfinite(r)) {
+            a.stopped[q] = JB_SOLVE_NON_FINITE;
+            fin = true;
+          } else if (r > a.tol && a.best[q] > 0.0 && r > a.diverge * a.best[q]) {
+            a.stopped[q] = JB_SOLVE_DIVERGING;
+            fin = true;
+          } else {
+            a.best[q] = fmin(a.best[q], r);
+            fin = r <= a.tol;
+          }
+        }
+        done = done && fin;
+      }
+      if (done || o >= a.max_outer || force)
+        act = 0;
+      else
+        a.outer[p] = o + 1;
+      a.active[p] = act;
+    }
+    cudaGraphSetConditional(a.ifh[p], act ? 1u : 0u);
+    if (act) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cudaGraphSetConditional(a.wh, any ? 1u : 0u);
+    *a.steps += 1;
+  }
+}
+
+// One graph launch for the whole batched run: while (any problem active) {
+// decide; for each problem: if (active) { correction; FP64 residual } }.
+// The first residuals and all lazily built tables come before (on `st`).
+// Returns JB_ESTATE when this CUDA build cannot make conditional nodes (the
+// caller then runs the per-step loop); fills outer / outc / residuals.
+int batch_persistent(jb_batch* B, void* const* eps, int max_outer, int inner, double tol,
+                     const std::vector<int64_t>& hoff, double* residuals,
+                     std::vector<int>& outer, std::vector<Outcome>& outc, cudaStream_t st) {
+  const int P = (int)B->prob.size();
+  const int nres = (int)B->nres;
+  const int64_t nhist = hoff.empty() ? 0 : hoff.back() + (int64_t)max_outer * B->prob.back()->L;
+  // device state: L, roff, hoff, active, outer, stopped, steps | best, last, hist | handles
+  auto al8 = [](size_t v) { return (v + 7) / 8 * 8; };
+  const size_t o_L = 0, o_roff = al8(o_L + 4 * P), o_hoff = al8(o_roff + 4 * P),
+               o_act = al8(o_hoff + 8 * P), o_out = al8(o_act + 4 * P),
+               o_stop = al8(o_out + 4 * P), o_steps = al8(o_stop + 4 * nres),
+               o_best = al8(o_steps + 8), o_last = al8(o_best + 8 * nres),
+               o_hist = al8(o_last + 8 * nres), o_h = al8(o_hist + 8 * nhist),
+               total = o_h + 8 * (P + 1);
+  JB_TRY(ensure_buf(B->dstate, total));
+  std::vector<unsigned char> host(total, 0);
+  auto put = [&](size_t off, const void* src, size_t bytes) {
+    std::memcpy(host.data() + off, src, bytes);
+  };
+  std::vector<int> Ls(P), roff(P), ones(P, 1);
+  for (int i = 0; i < P; ++i) {
+    Ls[i] = B->prob[i]->L;
+    roff[i] = (int)B->res_off[i];
+  }
+  std::vector<double> inf(nres, INFINITY);
+  put(o_L, Ls.data(), 4 * P);
+  put(o_roff, roff.data(), 4 * P);
+  put(o_hoff, hoff.data(), 8 * P);
+  put(o_act, ones.data(), 4 * P);
+  put(o_out, ones.data(), 4 * P);
+  put(o_best, inf.data(), 8 * nres);
+  put(o_last, inf.data(), 8 * nres);
+  unsigned char* d = static_cast<unsigned char*>(B->dstate.p);
+
+  cudaGraph_t g = nullptr;
+  JB_CUDA(cudaGraphCreate(&g, 0));
+  std::vector<cudaGraphConditionalHandle> h(P + 1);
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h[P], g, 1, cudaGraphCondAssignDefault);
+  for (int i = 0; i < P && e == cudaSuccess; ++i)
+    e = cudaGraphConditionalHandleCreate(&h[i], g, 0, 0);
+  cudaGraphNode_t wnode = nullptr;
+  cudaGraphNodeParams wp = {};
+  if (e == cudaSuccess) {
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = h[P];
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    e = cudaGraphAddNode(&wnode, g, nullptr, 0, &wp);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return fail(JB_ESTATE, std::string("conditional graph nodes unavailable: ") +
+                               cudaGetErrorString(e));
+  }
+  put(o_h, h.data(), 8 * (P + 1));
+  JB_CUDA(cudaMemcpyAsync(d, host.data(), total, cudaMemcpyHostToDevice, st));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  cudaStream_t cs = B->streams[1 % B->streams.size()];
+  BatchDecide dk;
+  dk.P = P;
+  dk.max_outer = max_outer;
+  dk.tol = tol;
+  dk.diverge = kDivergeFactor;
+  dk.L = reinterpret_cast<const int*>(d + o_L);
+  dk.roff = reinterpret_cast<const int*>(d + o_roff);
+  dk.hoff = reinterpret_cast<const int64_t*>(d + o_hoff);
+  dk.res = static_cast<const double*>(B->res_all.p);
+  dk.hist = reinterpret_cast<double*>(d + o_hist);
+  dk.best = reinterpret_cast<double*>(d + o_best);
+  dk.last = reinterpret_cast<double*>(d + o_last);
+  dk.stopped = reinterpret_cast<int*>(d + o_stop);
+  dk.active = reinterpret_cast<int*>(d + o_act);
+  dk.outer = reinterpret_cast<int*>(d + o_out);
+  dk.steps = reinterpret_cast<int*>(d + o_steps);
+  dk.ifh = reinterpret_cast<const cudaGraphConditionalHandle*>(d + o_h);
+  dk.wh = h[P];
+  // the body: the decision kernel, then one IF node per problem after it
+  int r = JB_OK;
+  e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+  if (e == cudaSuccess) {
+    batch_decide_kernel<<<1, 256, 0, cs>>>(dk);
+    e = cudaGetLastError();
+    cudaGraph_t same = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cs, &same);
+    if (e == cudaSuccess) e = ee;
+  }
+  cudaGraphNode_t decide = nullptr;
+  size_t nn = 1;
+  if (e == cudaSuccess) e = cudaGraphGetNodes(body, &decide, &nn);
+  for (int i = 0; i < P && e == cudaSuccess && r == JB_OK; ++i) {
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = h[i];
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode = nullptr;
+    e = cudaGraphAddNode(&inode, body, &decide, 1, &ip);
+    if (e != cudaSuccess) break;
+    e = cudaStreamBeginCaptureToGraph(cs, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) break;
+    jb_mixed* M = B->prob[i];
+    r = M->method != JB_INNER_BASIC ? mixed_correct_bicgstab(M, eps[i], inner, cs)
+                                    : mixed_correct(M, eps[i], inner, cs);
+    if (r == JB_OK)
+      r = mixed_residual(M, eps[i], static_cast<double*>(B->res_all.p) + B->res_off[i], cs);
+    cudaGraph_t same = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cs, &same);
+    if (e == cudaSuccess) e = ee;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess && r == JB_OK) e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (r != JB_OK) {
+    if (exec) cudaGraphExecDestroy(exec);
+    return r;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (exec) cudaGraphExecDestroy(exec);
+    return fail(JB_ESTATE, std::string("persistent batch graph: ") + cudaGetErrorString(e));
+  }
+  // after the eager work on the caller's stream, one launch runs to the end
+  JB_CUDA(cudaGraphLaunch(exec, st));
+  JB_CUDA(cudaMemcpyAsync(host.data(), d, total, cudaMemcpyDeviceToHost, st));
+  unsigned fault = 0;
+  JB_CUDA(jb::fetch_fault_async(&fault, st));
+  const cudaError_t se = cudaStreamSynchronize(st);
+  cudaGraphExecDestroy(exec);
+  JB_CUDA(se);
+  JB_TRY(check_fault(fault, "jb_batch_run"));
+  const int* outd = reinterpret_cast<const int*>(host.data() + o_out);
+  const int* stopd = reinterpret_cast<const int*>(host.data() + o_stop);
+  const double* bestd = reinterpret_cast<const double*>(host.data() + o_best);
+  const double* lastd = reinterpret_cast<const double*>(host.data() + o_last);
+  const double* histd = reinterpret_cast<const double*>(host.data() + o_hist);
+  for (int i = 0; i < P; ++i) {
+    outer[i] = outd[i];
+    for (int l = 0; l < Ls[i]; ++l) {
+      const int q = roff[i] + l;
+      outc[i].stopped[l] = stopd[q];
+      outc[i].best[l] = bestd[q];
+      outc[i].last[l] = lastd[q];
+    }
+  }
+  if (residuals) std::memcpy(residuals, histd, 8 * (size_t)nhist);
+  return JB_OK;
+}
+
+}  // namespace
+
 extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int init,
                             int max_outer, int inner, double tol, double* residuals,
                             int* outer_out, int* fp32_iters_out, double* mean_tau,
@@ -2273,7 +2514,21 @@ extern "C" int jb_batch_run(jb_batch* B, const double* E, void* const* eps, int 
   for (size_t i = 0; i < P; ++i) outc.emplace_back(B->prob[i]->L);
   unsigned fault = 0;
   int launches = 0;
-  for (int step = 0;; ++step) {
+  bool done_persistent = false;
+  if (B->persistent) {
+    std::vector<int64_t> hoff(hist_off.begin(), hist_off.end());
+    const int pr = batch_persistent(B, eps, max_outer, inner, tol, hoff, residuals, outer, outc,
+                                    st);
+    if (pr == JB_OK) {
+      done_persistent = true;
+      launches = 1;
+    } else if (pr == JB_ESTATE) {
+      B->persistent = false;  // this CUDA build: the per-step loop from now on
+    } else {
+      return pr;
+    }
+  }
+  for (int step = 0; !done_persistent; ++step) {
     cudaStream_t rs = step == 0 ? st : origin;
     JB_CUDA(cudaMemcpyAsync(rh.data(), res, sizeof(double) * B->nres, cudaMemcpyDeviceToHost,
                             rs));

@@ -44,7 +44,14 @@ def test_batch_matches_one_by_one(variant):
     E = [np.eye(3) for _ in probs]
     batch = BatchedMixedScheme([(g, l, 3) for g, l in ops_], inner=20, branches=4)
     res = batch.run(E, tol=1e-8, max_outer=2000)
-    assert batch.graph_launches == max(r.outer_iterations for r in res) - 1
+    assert batch.graph_launches == 1   # the whole run in one persistent graph launch
+    step = BatchedMixedScheme([(g, l, 3) for g, l in ops_], inner=20, branches=4,
+                              persistent=False)
+    res_step = step.run(E, tol=1e-8, max_outer=2000)
+    assert step.graph_launches == max(r.outer_iterations for r in res) - 1
+    for r, q in zip(res, res_step):
+        assert torch.equal(r.eps, q.eps) and np.array_equal(r.residuals, q.residuals)
+        assert list(r.status) == list(q.status)
     for (g, l), r in zip(ops_, res):
         one = MixedScheme(g, l, 3, inner=20).run(np.eye(3), tol=1e-8, max_outer=2000)
         assert r.outer_iterations == one.outer_iterations
