@@ -125,3 +125,37 @@ def test_batch_bicgstab_matches_one_by_one():
         assert r.fp32_iterations == one.fp32_iterations
         assert torch.equal(r.eps, one.eps)
         assert r.residuals[-1].max() <= 1e-9
+
+
+@pytest.mark.gpu
+def test_batch_config3_range_long_axes():
+    """The batched workload's own range: grids of 384 to 1024 points a side
+    (the long-axis Green pass), contrasts up to 1000, 3 load cases, BiCGSTAB
+    corrections: bitwise equal to the same cells solved one by one, one
+    graph launch, and effective stiffness within 1e-7 of FP64 GMRES on the
+    FP64 equation."""
+    from janus_b200.solvers import GMRES
+    probs = micro.batch_2d_problems(4, seed=11, sizes=(384, 512, 768, 1024))
+    probs[0]["mu"][1] = 1000.0          # the top of the contrast range
+    for p in probs:
+        k = p["mu"] / (1 - 2 * p["nu"])
+        p["mu0"] = 0.5 * (p["mu"][0] + p["mu"][1])
+        k0 = 0.5 * (k.min() + k.max())
+        p["nu0"] = (k0 - p["mu0"]) / (2 * k0)
+    ops_ = [_operators(p, "filtered") for p in probs]
+    tol = 1e-9
+    batch = BatchedMixedScheme([(g, l, 3) for g, l in ops_], inner=25, method="bicgstab")
+    res = batch.run([np.eye(3)] * len(probs), tol=tol, max_outer=100)
+    assert batch.graph_launches == 1
+    for p, (g, l), r in zip(probs, ops_, res):
+        assert r.converged and r.residuals[-1].max() <= tol
+        one = MixedScheme(g, l, 3, inner=25, method="bicgstab_fixed").run(
+            np.eye(3), tol=tol, max_outer=100)
+        assert r.outer_iterations == one.outer_iterations
+        assert torch.equal(r.eps, one.eps)
+        ref = GMRES(g, l, nload=3, restart=20).run(np.eye(3), tol=1e-11, max_iter=20000)
+        assert ref.converged
+        mat0 = material.create(p["mu0"], p["nu0"], 2)
+        c_ref = ref.mean_stress(mat0, np.eye(3))
+        c_mix = r.mean_stress(mat0, np.eye(3))
+        assert np.abs(c_mix - c_ref).max() <= 1e-7 * np.abs(c_ref).max()
