@@ -1,7 +1,9 @@
 """Failure reporting of the solvers and the pass kernels, in the forms that
 fault no GPU: non-finite and diverging load cases are made on the host (a
-NaN in the macroscopic strain or the phase table, a reference medium that
-makes the basic scheme diverge), and a timed-out copy wait is made by
+NaN in one load case's initial strain field or in the phase table, a
+reference medium that makes the basic scheme diverge; a NaN macroscopic
+strain is rejected before any work as an invalid argument), and a
+timed-out copy wait is made by
 lowering the first bounded wait to one poll, after which every kernel drains
 its own copy at the full limit and returns.
 
@@ -9,6 +11,7 @@ No counterpart in the reference, whose tutorial loop only records the
 residuals (sphinx/tutorials/square_basic/square_basic.py:88-92)."""
 import numpy as np
 import pytest
+import torch
 
 import janus_b200.material.elastic.linear.isotropic as material
 from janus_b200 import _lib
@@ -35,12 +38,24 @@ def _problem(phase, mats, g0, nu0, variant="truncated", nan_phase=None):
     return loc, green
 
 
+def _nan_start(shape, E):
+    """initial fields: E everywhere, load case 1 poisoned at one voxel"""
+    eps = torch.empty(shape, dtype=torch.float64, device="cuda")
+    eps[...] = torch.from_numpy(E).cuda().view((E.shape[0],) + (1,) * (len(shape) - 2) +
+                                                (E.shape[1],))
+    eps[(1,) + (0,) * (len(shape) - 1)] = float("nan")
+    return eps
+
+
 @pytest.mark.gpu
 def test_basic_scheme_nan_load_case_stops_at_once():
     phase = micro.square_inclusion(64, side=32)
     loc, green = _problem(phase, [(1.0, 0.3), (10.0, 0.3)], 5.5, 0.3)
-    E = np.array([[0.0, 0.0, 1.0], [np.nan, 0.0, 0.0]])
-    r = BasicScheme(green, loc, nload=2).run(E, 500, tol=1e-8)
+    E = np.array([[0.0, 0.0, 1.0], [1.0, 0.0, 0.0]])
+    s = BasicScheme(green, loc, nload=2)
+    with pytest.raises(ValueError, match="nonzero"):
+        s.run(np.array([[0.0, 0.0, 1.0], [np.nan, 0.0, 0.0]]), 10)
+    r = s.run(E, 500, tol=1e-8, eps=_nan_start(s.field_shape, E), init=False)
     assert list(r.status) == [CONVERGED, NON_FINITE]
     assert r.status_names == ["converged", "non_finite"]
     assert not r.converged
@@ -78,8 +93,9 @@ def test_mixed_scheme_statuses():
     loc, green = _problem(phase, [(1.0, 0.3), (10.0, 0.3)], 5.5, 0.3, "filtered")
     E = np.zeros((2, 6))
     E[0, 0] = 1.0
-    E[1, 2] = np.nan
-    r = MixedScheme(green, loc, nload=2, inner=10).run(E, tol=1e-10, max_outer=100)
+    E[1, 2] = 1.0
+    m = MixedScheme(green, loc, nload=2, inner=10)
+    r = m.run(E, tol=1e-10, max_outer=100, eps=_nan_start(m.field_shape, E))
     assert list(r.status) == [CONVERGED, NON_FINITE]
     # diverging: the FP64 residual of the basic scheme grows outer step by outer step
     loc, green = _problem(phase, [(1.0, 0.3), (100.0, 0.3)], 10.0, 0.3, "filtered")
@@ -108,9 +124,12 @@ def test_batch_statuses_per_problem():
     loc1, g1 = _problem(micro.square_inclusion(48, side=16), [(1.0, 0.3), (100.0, 0.3)], 10.0,
                         0.3)
     b = BatchedMixedScheme([(g0, loc0, 2), (g1, loc1, 1)], inner=6)
-    E0 = np.array([[0.0, 0.0, 1.0], [np.nan, 0.0, 0.0]])
+    E0 = np.array([[0.0, 0.0, 1.0], [1.0, 0.0, 0.0]])
     E1 = np.array([[1.0, 0.0, 0.0]])
-    out = b.run([E0, E1], tol=1e-9, max_outer=80)
+    e1 = torch.empty(b.schemes[1].field_shape, dtype=torch.float64, device="cuda")
+    e1[...] = torch.from_numpy(E1).cuda().view(1, 1, 1, 3)
+    out = b.run([E0, E1], tol=1e-9, max_outer=80,
+                eps=[_nan_start(b.schemes[0].field_shape, E0), e1])
     assert list(out[0].status) == [CONVERGED, NON_FINITE]
     assert list(out[1].status) == [DIVERGING]
 
