@@ -78,12 +78,12 @@ int jb_max_axis_length(int dtype);
  * code).  Synchronises with the device. */
 int jb_device_status(unsigned *fault);
 /* Polls of the first bounded wait of every asynchronous copy in the pass
- * kernels (0 restores the default, 2^24).  For tests of the failure path
- * only: a small value makes the first wait give up while the copy is still
- * in flight; the kernel then sets the fault word, waits at the full limit
- * for its own copy and returns, and the solvers report JB_EFAULT at their
- * next synchronisation.  No reference counterpart. */
-int jb_set_wait_limit(unsigned polls);
+ * kernels (a negative value restores the default, 2^24).  For tests of the
+ * failure path only: 0 makes every first wait give up at once, while its
+ * copy is still in flight; the kernel then sets the fault word, waits at the
+ * full limit for its own copy and returns, and the solvers report JB_EFAULT
+ * at their next synchronisation.  No reference counterpart. */
+int jb_set_wait_limit(int polls);
 
 /* ---- real FFT objects ------------------------------------------------- */
 

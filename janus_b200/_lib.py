@@ -43,7 +43,7 @@ _SIGS = {
     "jb_last_error": ([], ctypes.c_char_p),
     "jb_max_axis_length": ([c_int], c_int),
     "jb_device_status": ([ctypes.POINTER(ctypes.c_uint)], c_int),
-    "jb_set_wait_limit": ([ctypes.c_uint], c_int),
+    "jb_set_wait_limit": ([c_int], c_int),
     "jb_fft_create": ([c_int, P_int64, c_int, ctypes.c_uint, ctypes.POINTER(c_void_p)], c_int),
     "jb_fft_destroy": ([c_void_p], c_int),
     "jb_fft_r2c": ([c_void_p, c_void_p, P_int64, c_void_p, c_void_p], c_int),
@@ -149,10 +149,11 @@ def check_device(what: str = "janus_b200") -> None:
                            f"copies (device fault word {f}); its results are invalid")
 
 
-def set_wait_limit(polls: int) -> None:
-    """Polls of the first bounded wait of every asynchronous copy (0: the
-    default).  For tests of the failure path."""
-    check(lib().jb_set_wait_limit(int(polls)))
+def set_wait_limit(polls=None) -> None:
+    """Polls of the first bounded wait of every asynchronous copy (None: the
+    default; 0: every first wait gives up at once).  For tests of the failure
+    path."""
+    check(lib().jb_set_wait_limit(-1 if polls is None else int(polls)))
 
 
 def status_names(status) -> list:

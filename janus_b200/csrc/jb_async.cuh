@@ -23,8 +23,8 @@ __device__ unsigned int g_jb_fault = 0;
 constexpr unsigned kWaitLimit = 1u << 24;
 
 // polls of the first bounded wait (kWaitLimit unless lowered through
-// jb_set_wait_limit to exercise the failure path in tests; the drain wait
-// after a timeout always keeps kWaitLimit)
+// jb_set_wait_limit to exercise the failure path in tests, 0: give up at
+// once; the drain wait after a timeout always keeps kWaitLimit)
 __constant__ unsigned c_jb_wait_first = kWaitLimit;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

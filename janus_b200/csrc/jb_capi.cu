@@ -502,7 +502,7 @@ int jb_device_status(unsigned* fault) {
   return JB_OK;
 }
 
-int jb_set_wait_limit(unsigned polls) {
+int jb_set_wait_limit(int polls) {
   JB_CUDA(jb::set_first_wait_limit(polls));
   return JB_OK;
 }

@@ -1,35 +1,45 @@
-// Axis-0 Green pass with a register-resident middle stage (sm_100a).
+// Axis-0 Green pass (sm_100a): each column of the half spectrum
+// [L][n0][F][C] (complex, F coefficients of C Mandel components per row) goes
+// through the forward transform along axis 0, every coefficient is contracted
+// with the discrete Green operator, and the column is transformed back: the
+// work of janus/green.pyx:356-390 (DiscreteGreenOperator3D.c_apply, axis-0
+// part) and 185-216 (2D).  One HBM round trip per value; the result is
+// unnormalised (the c2r pass scales by 1/N, as
+// janus/fft/serial/_serial_fft.pyx:121-150 does).
 //
-// The pass takes each column of the half spectrum [L][n0][F][C] (complex,
-// F coefficients of C Mandel components per row) through the forward
-// transform along axis 0, contracts every coefficient with the discrete
-// Green operator, and transforms back: the work of janus/green.pyx:356-390
-// (DiscreteGreenOperator3D.c_apply, axis-0 part) and 185-216 (2D).
+// n0 = 32 ... 256: five-phase tiles.  n0 = N1 N2 is split as n = j + N2 m,
+// k = k1 + N1 k2:
+//   X[k1 + N1 k2] = sum_j w_N2^(j k2) [w_n0^(j k1) sum_m x[j + N2 m] w_N1^(m k1)].
+// A tile is one load case, 6 NG columns (NG 6-column groups: one 3D
+// coefficient or two 2D ones each) and all n0 rows, in shared memory as
+// S[k1][j][c].
+//   P1 (lane per column c and j): the N1 values x[j + N2 m] from global
+//      memory, the N1-point transform in registers, the twiddles
+//      w_n0^(j k1), to S[k1][j][c].
+//   2a (lane per k1 and c): the N2-point transform over j in registers, in
+//      place (j becomes k2).
+//   2b (lane per k1, k2 and group): the group's components at
+//      b0 = k1 + N1 k2 contracted with the operator (a symmetric Mandel
+//      matrix from the table, or on the fly), in place.
+//   2c: the inverse of 2a; P3: the conjugate twiddles, the inverse of P1's
+//      transform and the store to global memory.
+// Every transform is a compile-time sequence in one lane's registers (no
+// shuffles); the phases hand values over through shared memory, four
+// barriers per tile.  P3 reads exactly the positions its own lane's P1 of
+// the next tile writes, so no barrier separates them.  The lanes use at most
+// 85 registers (128 where both transforms hold 16 values), so that three
+// CTAs of 256 threads share an SM.
 //
-// n0 = 4 NL is split as n = j + 4 m (j < 4, m < NL), k = k1 + NL k2:
-//   X[k1 + NL k2] = sum_j w4^(j k2) w_n0^(j k1) sum_m x[j + 4 m] w_NL^(m k1).
-// Phase 1: the lanes of a (load case, column, j) slice load its NL values of
-//          the column straight from global memory into registers and compute
-//          the NL-point transform over m in registers: one lane for NL <= 16;
-//          for NL = 16 S, S lanes (m = a + S b), each a 16-point transform
-//          of its rows, a twiddle, then an S-point transform across the
-//          lanes by shuffles (S = 2: one radix-2 step with compile-time
-//          twiddles; S = 4..16: radix-2 steps and a bit-reversal exchange);
-//          then the NL results go to shared memory.
-// Phase 2: one thread per (load case, k1, group of 6 columns: one 3D
-//          coefficient or two 2D ones) reads its 4 x 6 values, applies the
-//          twiddles w_n0^(j k1) and the 4-point transform over j, contracts
-//          the Green operator at the 4 rows b0 = k1 + NL k2 in registers,
-//          transforms back and writes the 4 x 6 values in place.
-// Phase 3: the phase-1 lanes read their values, transform back and store
-//          the column to global memory.
-// Each spectral value therefore crosses shared memory twice each way and is
-// read and written once in HBM.  Up to n0 = 256 a tile holds two load cases
-// of the same coefficients, so the two lanes of a phase-2 pair read the same
-// table entries in one broadcast.  The next tile's rows are prefetched into L2
-// while the current tile is transformed.  There are no waits besides the
-// block barriers.  The result is unnormalised (the c2r pass scales by 1/N,
-// as janus/fft/serial/_serial_fft.pyx:121-150 does).
+// n0 = 512, 1024: lane-split tiles.  n0 = 4 NL, n = j + 4 m, k = k1 + NL k2;
+// phase 1: the S = NL/16 lanes of a (column, j) slice each load 16 values
+// (m = a + S b), transform them in registers, apply w_NL^(a e) and finish
+// the NL-point transform across the S lanes by shuffles (radix-2 steps and a
+// bit-reversal exchange); phase 2: one lane per (k1, group) applies the
+// twiddles w_n0^(j k1), the 4-point transform over j, the contraction at the
+// four rows b0 = k1 + NL k2, and the inverse; phase 3 mirrors phase 1.  The
+// next tile's rows are prefetched into L2 while a tile is transformed.
+//
+// No waits besides the block barriers.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -39,183 +49,7 @@
 namespace jb {
 namespace {
 
-// cos(pi e / 16), e = 0..8 (correctly rounded to double)
-__host__ __device__ constexpr double cospi16(int e) {
-  return e == 0   ? 1.0
-         : e == 1 ? 0.98078528040323044912618223613424
-         : e == 2 ? 0.92387953251128675612818318939679
-         : e == 3 ? 0.83146961230254523707878837761791
-         : e == 4 ? 0.70710678118654752440084436210485
-         : e == 5 ? 0.55557023301960222474283081394853
-         : e == 6 ? 0.38268343236508977172845998403040
-         : e == 7 ? 0.19509032201612826784828486847702
-                  : 0.0;
-}
-// forward twiddle w32^e = exp(-2 pi i e / 32) = (cos(pi e/16), -sin(pi e/16)), e < 16
-template <typename T> __device__ __forceinline__ constexpr T w32_re(int e) {
-  return e <= 8 ? T(cospi16(e)) : T(-cospi16(16 - e));
-}
-template <typename T> __device__ __forceinline__ constexpr T w32_im(int e) {
-  return e <= 8 ? T(-cospi16(8 - e)) : T(-cospi16(e - 8));
-}
-
-// multiply by w32^e (DIR -1) or its conjugate (DIR +1) where `on` (the odd
-// lane of a pair), by 1 elsewhere: a per-lane selection instead of a
-// divergent branch
-template <int DIR, int E, typename C> __device__ __forceinline__ C rot32_if(C a, bool on) {
-  using T = decltype(a.x);
-  if constexpr (E == 0) {
-    return a;
-  } else {
-    const T c = on ? w32_re<T>(E) : T(1);
-    const T s = on ? (DIR < 0 ? w32_im<T>(E) : -w32_im<T>(E)) : T(0);
-    return mkc(a.x * c - a.y * s, a.y * c + a.x * s);
-  }
-}
-
-template <typename C> __device__ __forceinline__ C shfl_xor1(C v) {
-  return mkc(__shfl_xor_sync(0xffffffffu, v.x, 1), __shfl_xor_sync(0xffffffffu, v.y, 1));
-}
-
-// lanes per column slice and values a lane holds: NL <= 16 is held by one
-// lane; NL = 16 S (S = 2, 4, 8, 16) is split over S consecutive lanes of a
-// warp, 16 values each, m = a + S b for lane a
-template <int NL> struct LaneSplit {
-  static constexpr int SPL = NL <= 16 ? 1 : NL / 16;
-  static constexpr int V = NL / SPL;
-};
-
-// row (relative to j) of value i of lane a (n = j + 4 m)
-template <int NL> __device__ __forceinline__ int lane_row(int i, int a) {
-  return 4 * (a + LaneSplit<NL>::SPL * i);
-}
-
-template <int E, typename C> struct PairLoop {
-  // forward: v[e] = U_a[e] -> Y[e + 16 a], with Y[e] = U0 + w32^e U1 and
-  // Y[e + 16] = U0 - w32^e U1
-  __device__ __forceinline__ static void fwd(C* v, bool odd) {
-    const C u = rot32_if<-1, E>(v[E], odd);
-    const C o = shfl_xor1(u);
-    v[E] = odd ? csub(o, u) : cadd(u, o);
-    PairLoop<E + 1, C>::fwd(v, odd);
-  }
-  // inverse: v[e] = V[e + 16 a] -> lane 0: V[e] + V[e + 16], lane 1:
-  // conj(w32^e) (V[e] - V[e + 16])
-  __device__ __forceinline__ static void inv(C* v, bool odd) {
-    const C u = v[E];
-    const C o = shfl_xor1(u);
-    v[E] = odd ? rot32_if<+1, E>(csub(o, u), true) : cadd(u, o);
-    PairLoop<E + 1, C>::inv(v, odd);
-  }
-};
-template <typename C> struct PairLoop<16, C> {
-  __device__ __forceinline__ static void fwd(C*, bool) {}
-  __device__ __forceinline__ static void inv(C*, bool) {}
-};
-
-template <int S> __device__ __forceinline__ int bit_reverse(int x) {
-  int r = 0;
-#pragma unroll
-  for (int m = 1; m < S; m <<= 1) {
-    r = (r << 1) | (x & 1);
-    x >>= 1;
-  }
-  return r;
-}
-
-// S-point DFT across the S lanes of a slice (S = 4, 8, 16) for each of the
-// 16 values: lane a holds V_a[e]; on return lane d holds
-// sum_a w_S^(DIR a d) V_a[e].  Radix-2 decimation in frequency over the lane
-// index (the lower lane of a pair keeps u + o, the upper (o - u) w_2h^q,
-// q = a mod h), then a bit-reversal permutation of the lanes.  tw: the
-// axis table exp(-2 pi i t / n0), n0 = 64 S.
-template <int S, int DIR, typename C>
-__device__ __forceinline__ void cross_lane_dft(C* v, int a, const C* tw) {
-  constexpr int N0 = 64 * S;
-#pragma unroll
-  for (int h = S / 2; h >= 1; h >>= 1) {
-    const bool upper = (a & h) != 0;
-    C w = tw[(a % h) * (N0 / (2 * h))];
-    if (DIR > 0) w = cconj(w);
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      const C u = v[e];
-      const C o = mkc(__shfl_xor_sync(0xffffffffu, u.x, h), __shfl_xor_sync(0xffffffffu, u.y, h));
-      v[e] = upper ? cmul(csub(o, u), w) : cadd(u, o);
-    }
-  }
-  const int src = ((threadIdx.x & 31) & ~(S - 1)) | bit_reverse<S>(a);
-#pragma unroll
-  for (int e = 0; e < 16; ++e)
-    v[e] = mkc(__shfl_sync(0xffffffffu, v[e].x, src), __shfl_sync(0xffffffffu, v[e].y, src));
-}
-
-// forward transform over m of a column slice: on entry v[i] holds row
-// j + 4 m(i, a); on return v[i] = Y[k1] at k1 = i + V a
-template <int NL, typename C>
-__device__ __forceinline__ void lane_fwd(C* v, int a, const C* tw) {
-  constexpr int S = LaneSplit<NL>::SPL;
-  if constexpr (S == 1) {
-    Dft<NL, -1, C>::run(v);
-  } else if constexpr (S == 2) {
-    Dft<16, -1, C>::run(v);
-    PairLoop<0, C>::fwd(v, a != 0);
-  } else {
-    Dft<16, -1, C>::run(v);
-    // V_a[e] = w_NL^(a e) U_a[e], w_NL = w_n0^4
-#pragma unroll
-    for (int e = 1; e < 16; ++e) v[e] = cmul(v[e], tw[4 * a * e]);
-    cross_lane_dft<S, -1>(v, a, tw);
-  }
-}
-
-// inverse: v[i] = V[k1] at k1 = i + V a -> v[i] = x at row j + 4 m(i, a)
-template <int NL, typename C>
-__device__ __forceinline__ void lane_inv(C* v, int a, const C* tw) {
-  constexpr int S = LaneSplit<NL>::SPL;
-  if constexpr (S == 1) {
-    Dft<NL, +1, C>::run(v);
-  } else if constexpr (S == 2) {
-    PairLoop<0, C>::inv(v, a != 0);
-    Dft<16, +1, C>::run(v);
-  } else {
-    cross_lane_dft<S, +1>(v, a, tw);
-#pragma unroll
-    for (int e = 1; e < 16; ++e) v[e] = cmulc(v[e], tw[4 * a * e]);
-    Dft<16, +1, C>::run(v);
-  }
-}
-
-// tile geometry for n0 = 4 NL (3D: C = 6, a 6-column group is one
-// coefficient; 2D: C = 3, two coefficients)
-template <typename T, int DIM, int NL> struct R4Tile {
-  static constexpr int C = DIM == 3 ? 6 : 3;
-  static constexpr int LT = NL <= 64 ? 2 : 1;     // load cases per tile
-  static constexpr int NG = NL <= 64 ? 128 / (LT * NL) : 1;  // 6-column groups per tile
-  static constexpr int WC = 6 * NG;               // columns per tile
-  static constexpr int SPL = LaneSplit<NL>::SPL;
-  static constexpr int P1 = LT * WC * 4 * SPL;    // phase-1/3 threads
-  static constexpr int P2 = LT * NL * NG;         // phase-2 threads
-  static constexpr int THREADS = P1 > P2 ? P1 : P2;
-  static constexpr int P = 4 * WC + 1;            // k1 stride (odd)
-  // shared-memory phases: 8 lanes of 16 bytes (FP64), 16 of 8 bytes (FP32)
-  static constexpr int LMOD = sizeof(T) == 8 ? 8 : 16;
-  // block d of 16 values (lane d of a split slice) sits d OSTEP further on,
-  // so that the lanes of a slice write disjoint banks
-  static constexpr int OSTEP = SPL == 1 ? 0 : (SPL >= LMOD ? 1 : LMOD / SPL);
-  // load-case stride: past the last value, and LMOD/2 mod LMOD, so that the
-  // two load cases of a phase-2 lane pair fall in disjoint banks
-  static constexpr int LS0 = NL * P + SPL * OSTEP;
-  static constexpr int LS = LS0 + ((LMOD / 2 - LS0 % LMOD) + LMOD) % LMOD;
-  static constexpr size_t SMEM = (size_t)LT * LS * sizeof(cx<T>);
-  // resident CTAs asked of the register allocator
-  static constexpr int MINB = THREADS > 256 ? 1 : (sizeof(T) == 8 ? 2 : 3);
-};
-
-// offset of value k1 in a (load case, j, column) slice
-template <typename K> __device__ __forceinline__ int k1_off(int k1) {
-  return k1 * K::P + (k1 >> 4) * K::OSTEP;
-}
+// ---- shared by both tile kinds ----
 
 template <typename T> struct Axis0Args {
   const cx<T>* in;
@@ -226,13 +60,18 @@ template <typename T> struct Axis0Args {
   int64_t ncoef;     // F
   int64_t m_last;    // 3D: coefficient f = b1 * m_last + b2
   int L;
-  int prefetch;      // rows 16-byte aligned: prefetch the next tile into L2
+  int prefetch;      // rows 16-byte aligned (lane-split tiles: L2 prefetch)
   GreenTables<T> gt;
   const T* tab;      // symmetric Mandel matrices [f][c][b0], or nullptr: on the fly
 };
 
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+// the value, re-read each time: lane indices derived from it are recomputed
+// in each phase instead of being hoisted out of the tile loop and held in
+// registers throughout
+__device__ __forceinline__ int opaque(int x) {
+  int r;
+  asm volatile("mov.b32 %0, %1;" : "=r"(r) : "r"(x));
+  return r;
 }
 
 // the Green contraction of coefficient f at row b0 (te: its C components):
@@ -278,24 +117,345 @@ __device__ __forceinline__ void contract(const Axis0Args<T>& a, int64_t f, int b
   }
 }
 
+// index of entry (i, j) of a symmetric S x S matrix stored as its diagonal
+// then the upper triangle row by row (the layout g_apply reads)
+template <int S> __device__ __forceinline__ constexpr int gidx(int i, int j) {
+  const int lo = i < j ? i : j, hi = i < j ? j : i;
+  return lo == hi ? lo : S + lo * (S - 1) - lo * (lo - 1) / 2 + (hi - lo - 1);
+}
+
+// dst = G te for the coefficients of one 6-column group at row b0, written
+// component by component (only te and the operator values stay live); a
+// coefficient past the end is copied unchanged
+template <typename T, int DIM, bool TAB, typename C>
+__device__ __forceinline__ void contract_row(const Axis0Args<T>& a, int64_t fbase, int b0,
+                                             int n0, C* te, C* dst) {
+  constexpr int S = DIM == 3 ? 6 : 3;
+#pragma unroll
+  for (int h = 0; h < 6 / S; ++h) {
+    const int64_t f = fbase + h;
+    C* t = te + h * S;
+    if constexpr (TAB) {
+      if (f < a.ncoef) {
+        constexpr int NT = GSize<DIM>::value;
+        const T* g = a.tab + (size_t)f * NT * n0 + b0;
+        T gv[NT];
+#pragma unroll
+        for (int k = 0; k < NT; ++k) gv[k] = __ldg(g + (size_t)k * n0);
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+          T re = T(0), im = T(0);
+#pragma unroll
+          for (int j = 0; j < S; ++j) {
+            re = fma(gv[gidx<S>(i, j)], t[j].x, re);
+            im = fma(gv[gidx<S>(i, j)], t[j].y, im);
+          }
+          dst[h * S + i] = mkc(re, im);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < S; ++i) dst[h * S + i] = t[i];
+      }
+    } else {
+      if (f < a.ncoef) contract<T, DIM, false>(a, f, b0, n0, t);
+#pragma unroll
+      for (int i = 0; i < S; ++i) dst[h * S + i] = t[i];
+    }
+  }
+}
+
+int g_sm_count = 0;
+
+// persistent grid: the resident CTAs of every SM, at most one per tile
+template <typename KFn>
+int persistent_grid(KFn k, int threads, size_t smem, int64_t tiles) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        g_sm_count <= 0)
+      g_sm_count = 148;
+  }
+  const int64_t g = (int64_t)per_sm * g_sm_count;
+  return (int)(tiles < g ? tiles : g);
+}
+
+// ---- five-phase tiles (n0 = 32 ... 256) ----
+
+// Five-phase tile of one load case, 6 NG columns and all n0 = N1 N2 rows
+// (n = j + N2 m, k = k1 + N1 k2), in shared memory as S[k1][j][c] with row
+// (j) stride PJ = 6 NG and k1 stride PK = N2 PJ + pad: the pad (1 for FP64,
+// 2 for FP32 tiles of two groups, 1 otherwise) was found by an exhaustive
+// search of the bank conflicts of every phase's access pattern, all
+// conflict-free except one 2-way phase in FP32.
+template <int N0> struct R8Shape;
+template <> struct R8Shape<32> { static constexpr int N1 = 8, N2 = 4, NG = 4; };
+template <> struct R8Shape<64> { static constexpr int N1 = 8, N2 = 8, NG = 2; };
+template <> struct R8Shape<128> { static constexpr int N1 = 8, N2 = 16, NG = 2; };
+template <> struct R8Shape<256> { static constexpr int N1 = 16, N2 = 16, NG = 1; };
+
+template <typename T, int DIM, int N0> struct R8Tile {
+  static constexpr int N1 = R8Shape<N0>::N1, N2 = R8Shape<N0>::N2, NG = R8Shape<N0>::NG;
+  static constexpr int C = DIM == 3 ? 6 : 3;
+  static constexpr int WC = 6 * NG;        // columns
+  static constexpr int P1 = WC * N2;       // phase-1/3 lanes (c, j)
+  static constexpr int P2A = N1 * WC;      // phase-2a/2c lanes (k1, c)
+  static constexpr int P2B = N1 * N2 * NG; // contraction lanes (k1, k2, group)
+  static constexpr int THREADS = P1 > P2A ? (P1 > P2B ? P1 : P2B) : (P2A > P2B ? P2A : P2B);
+  static constexpr int PJ = WC;
+  static constexpr int PK = N2 * PJ + (sizeof(T) == 8 || NG != 2 ? 1 : 2);
+  static constexpr size_t SMEM = (size_t)N1 * PK * sizeof(cx<T>);
+  // resident CTAs asked of the register allocator: 24 warps per SM in FP64
+  // (at most 85 registers; 16 warps and 128 registers where both transform
+  // phases hold 16 values), 32 in FP32 (64 registers)
+  static constexpr int MINB =
+      (sizeof(T) == 8 ? (N1 == 16 && N2 == 16 ? 16 : 24) : 32) * 32 / THREADS;
+};
+
+template <typename T, int DIM, int N0, bool TAB>
+__global__ void __launch_bounds__(R8Tile<T, DIM, N0>::THREADS, R8Tile<T, DIM, N0>::MINB)
+    green_axis0_r8_kernel(Axis0Args<T> a) {
+  using C = cx<T>;
+  using K = R8Tile<T, DIM, N0>;
+  constexpr int N1 = K::N1, N2 = K::N2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* S = reinterpret_cast<C*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int LP = a.L;
+  const int64_t total = (a.inner + K::WC - 1) / K::WC * LP;
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const int64_t chunk = t / LP;
+    const int lg = (int)(t - chunk * LP);
+    const int64_t col0 = chunk * K::WC;
+    // P1: lane (c, j): N1-point transform over m, twiddles w_n0^(j k1)
+    if (tid < K::P1) {
+      const int tq = opaque(tid);
+      const int c = tq % K::WC, j = tq / K::WC;
+      const bool ok = col0 + c < a.inner;
+      C v[N1];
+      const int64_t pitch = a.pitch;
+      const C* src = a.in + ((int64_t)lg * N0 + j) * pitch + col0 + c;
+#pragma unroll
+      for (int m = 0; m < N1; ++m) v[m] = ok ? src[(int64_t)m * N2 * pitch] : mkc(T(0), T(0));
+      Dft<N1, -1, C>::run(v);
+      asm volatile("" ::: "memory");
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], a.tw[j * k1]);
+      C* s = S + j * K::PJ + c;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) s[k1 * K::PK] = v[k1];
+    }
+    __syncthreads();
+    // 2a: lane (k1, c): N2-point transform over j
+    if (tid < K::P2A) {
+      const int tq = opaque(tid);
+      C* s = S + (tq % N1) * K::PK + tq / N1;
+      C w[N2];
+#pragma unroll
+      for (int j = 0; j < N2; ++j) w[j] = s[j * K::PJ];
+      Dft<N2, -1, C>::run(w);
+#pragma unroll
+      for (int j = 0; j < N2; ++j) s[j * K::PJ] = w[j];
+    }
+    __syncthreads();
+    // 2b: lane (k1, k2, g2): the contraction at b0 = k1 + N1 k2
+    if (tid < K::P2B) {
+      const int tq = opaque(tid);
+      const int k1 = tq % N1, k2 = (tq / N1) % N2, g2 = tq / (N1 * N2);
+      C* s = S + k1 * K::PK + k2 * K::PJ + g2 * 6;
+      C y[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) y[q] = s[q];
+      contract_row<T, DIM, TAB>(a, (col0 + g2 * 6) / K::C, k1 + N1 * k2, N0, y, s);
+    }
+    __syncthreads();
+    // 2c: inverse over k2
+    if (tid < K::P2A) {
+      const int tq = opaque(tid);
+      C* s = S + (tq % N1) * K::PK + tq / N1;
+      C w[N2];
+#pragma unroll
+      for (int j = 0; j < N2; ++j) w[j] = s[j * K::PJ];
+      Dft<N2, +1, C>::run(w);
+#pragma unroll
+      for (int j = 0; j < N2; ++j) s[j * K::PJ] = w[j];
+    }
+    __syncthreads();
+    // P3: conj twiddles, inverse over k1, store (the next tile's P1 writes
+    // only the positions this lane reads here: no barrier)
+    if (tid < K::P1) {
+      const int tq = opaque(tid);
+      const int c = tq % K::WC, j = tq / K::WC;
+      C v[N1];
+      const C* s = S + j * K::PJ + c;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) v[k1] = s[k1 * K::PK];
+      asm volatile("" ::: "memory");
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulc(v[k1], a.tw[j * k1]);
+      Dft<N1, +1, C>::run(v);
+      if (col0 + c < a.inner) {
+        const int64_t pitch = a.pitch;
+        C* dst = a.out + ((int64_t)lg * N0 + j) * pitch + col0 + c;
+#pragma unroll
+        for (int m = 0; m < N1; ++m) __stcs(dst + (int64_t)m * N2 * pitch, v[m]);
+      }
+    }
+  }
+}
+
+template <typename T, int DIM, int N0, bool TAB>
+cudaError_t axis0_r8_go(const Axis0Args<T>& a, cudaStream_t st) {
+  using K = R8Tile<T, DIM, N0>;
+  auto k = &green_axis0_r8_kernel<T, DIM, N0, TAB>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)K::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int64_t tiles = (a.inner + K::WC - 1) / K::WC * a.L;
+  k<<<persistent_grid(k, K::THREADS, K::SMEM, tiles), K::THREADS, K::SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ---- lane-split tiles (n0 = 512, 1024) ----
+
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// lanes per column slice of the lane-split tiles: NL = 16 S is split over S
+// consecutive lanes of a warp, 16 values each, m = a + S b for lane a
+template <int NL> struct LaneSplit {
+  static_assert(NL >= 64 && NL % 16 == 0, "lane-split tiles: NL = 16 S, S >= 4");
+  static constexpr int SPL = NL / 16;
+  static constexpr int V = 16;
+};
+
+// row (relative to j) of value i of lane a (n = j + 4 m)
+template <int NL> __device__ __forceinline__ int lane_row(int i, int a) {
+  return 4 * (a + LaneSplit<NL>::SPL * i);
+}
+
+template <int S> __device__ __forceinline__ int bit_reverse(int x) {
+  int r = 0;
+#pragma unroll
+  for (int m = 1; m < S; m <<= 1) {
+    r = (r << 1) | (x & 1);
+    x >>= 1;
+  }
+  return r;
+}
+
+// S-point DFT across the S lanes of a slice (S = 4, 8, 16) for each of the
+// 16 values: lane a holds V_a[e]; on return lane d holds
+// sum_a w_S^(DIR a d) V_a[e].  Radix-2 decimation in frequency over the lane
+// index (the lower lane of a pair keeps u + o, the upper (o - u) w_2h^q,
+// q = a mod h, both as fma(sg, u, o) times a twiddle that is exactly 1 on the
+// lower lane), then a bit-reversal permutation of the lanes.  tw: the axis
+// table exp(-2 pi i t / n0), n0 = 64 S.
+template <int S, int DIR, typename C>
+__device__ __forceinline__ void cross_lane_dft(C* v, int a, const C* tw) {
+  using T = decltype(v[0].x);
+  constexpr int N0 = 64 * S;
+#pragma unroll
+  for (int h = S / 2; h >= 1; h >>= 1) {
+    const bool upper = (a & h) != 0;
+    asm volatile("" ::: "memory");  // one stage's twiddle live at a time
+    const C wt = tw[(a % h) * (N0 / (2 * h))];
+    const C w = upper ? (DIR > 0 ? cconj(wt) : wt) : mkc(T(1), T(0));
+    const T sg = upper ? T(-1) : T(1);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const C u = v[e];
+      const C o = mkc(__shfl_xor_sync(0xffffffffu, u.x, h), __shfl_xor_sync(0xffffffffu, u.y, h));
+      v[e] = cmul(mkc(fma(sg, u.x, o.x), fma(sg, u.y, o.y)), w);
+    }
+  }
+  const int src = ((threadIdx.x & 31) & ~(S - 1)) | bit_reverse<S>(a);
+#pragma unroll
+  for (int e = 0; e < 16; ++e)
+    v[e] = mkc(__shfl_sync(0xffffffffu, v[e].x, src), __shfl_sync(0xffffffffu, v[e].y, src));
+}
+
+// forward transform over m of a column slice: on entry v[i] holds row
+// j + 4 m(i, a); on return v[i] = Y[k1] at k1 = i + 16 a
+template <int NL, typename C>
+__device__ __forceinline__ void lane_fwd(C* v, int a, const C* tw) {
+  constexpr int S = LaneSplit<NL>::SPL;
+  Dft<16, -1, C>::run(v);
+  // V_a[e] = w_NL^(a e) U_a[e], w_NL = w_n0^4; the twiddles are read here,
+  // not ahead of the transform, where they would only hold registers
+  asm volatile("" ::: "memory");
+#pragma unroll
+  for (int e = 1; e < 16; ++e) v[e] = cmul(v[e], tw[4 * a * e]);
+  cross_lane_dft<S, -1>(v, a, tw);
+}
+
+// inverse: v[i] = V[k1] at k1 = i + 16 a -> v[i] = x at row j + 4 m(i, a)
+template <int NL, typename C>
+__device__ __forceinline__ void lane_inv(C* v, int a, const C* tw) {
+  constexpr int S = LaneSplit<NL>::SPL;
+  cross_lane_dft<S, +1>(v, a, tw);
+  asm volatile("" ::: "memory");
+#pragma unroll
+  for (int e = 1; e < 16; ++e) v[e] = cmulc(v[e], tw[4 * a * e]);
+  Dft<16, +1, C>::run(v);
+}
+
+// lane-split tile geometry for n0 = 4 NL (one load case, one 6-column group)
+template <typename T, int DIM, int NL> struct R4Tile {
+  static constexpr int C = DIM == 3 ? 6 : 3;
+  static constexpr int LT = 1;                    // load cases per tile
+  static constexpr int NG = 1;                    // 6-column groups per tile
+  static constexpr int WC = 6 * NG;               // columns per tile
+  static constexpr int SPL = LaneSplit<NL>::SPL;
+  static constexpr int P1 = LT * WC * 4 * SPL;    // phase-1/3 threads
+  static constexpr int P2 = LT * NL * NG;         // phase-2 threads
+  static constexpr int THREADS = P1 > P2 ? P1 : P2;
+  static constexpr int P = 4 * WC + 1;            // k1 stride (odd)
+  // shared-memory phases: 8 lanes of 16 bytes (FP64), 16 of 8 bytes (FP32)
+  static constexpr int LMOD = sizeof(T) == 8 ? 8 : 16;
+  // block d of 16 values (lane d of a split slice) sits d OSTEP further on,
+  // so that the lanes of a slice write disjoint banks
+  static constexpr int OSTEP = SPL >= LMOD ? 1 : LMOD / SPL;
+  static constexpr int LS = NL * P + SPL * OSTEP;
+  static constexpr size_t SMEM = (size_t)LT * LS * sizeof(cx<T>);
+  // resident CTAs asked of the register allocator
+  static constexpr int MINB = THREADS > 256 ? 1 : (sizeof(T) == 8 ? 2 : 3);
+};
+
+// offset of value k1 in a (load case, j, column) slice
+template <typename K> __device__ __forceinline__ int k1_off(int k1) {
+  return k1 * K::P + (k1 >> 4) * K::OSTEP;
+}
+
 template <typename T, int DIM, int NL, bool TAB>
 __global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL>::MINB)
     green_axis0_r4_kernel(Axis0Args<T> a) {
   using C = cx<T>;
   using K = R4Tile<T, DIM, NL>;
   constexpr int N0 = 4 * NL;
-  constexpr int NV = LaneSplit<NL>::V;
+  constexpr int NV = LaneSplit<NL>::V;  // 16
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* S = reinterpret_cast<C*>(smem_raw);
   const int tid = threadIdx.x;
-  // phase-1/3 lane: half a of a pair (pair split), column c, load case l1, j1
+  // phase-1/3 lane: lane a1 of a split slice, column c, load case l1, j1
   const bool p1 = tid < K::P1;
   const int a1 = tid % K::SPL;
   const int s1 = tid / K::SPL;
   const int c = s1 % K::WC;
   const int l1 = (s1 / K::WC) % K::LT;
   const int j1 = s1 / (K::WC * K::LT);
-  // phase-2 lane: load case l2 (fastest, so pairs share table loads), k1, group g2
+  // phase-2 lane: load case l2, k1, group g2
   const bool p2 = tid < K::P2;
   const int l2 = tid % K::LT;
   const int k1 = (tid / K::LT) % NL;
@@ -339,7 +499,8 @@ __global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL
         v[i] = ok1 ? src[(int64_t)lane_row<NL>(i, a1) * pitch] : mkc(T(0), T(0));
       lane_fwd<NL>(v, a1, a.tw);
     }
-    __syncthreads();  // the previous tile's phase 3 has read S
+    // (no barrier: phase 3 of the previous tile read these positions in
+    // this same lane)
     if (p1) {
       C* s = S + l1 * K::LS + j1 * K::WC + c;
 #pragma unroll
@@ -409,10 +570,8 @@ __global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL
   }
 }
 
-int g_sm_count = 0;
-
 template <typename T, int DIM, int NL, bool TAB>
-cudaError_t axis0_go(const Axis0Args<T>& a, cudaStream_t st) {
+cudaError_t axis0_r4_go(const Axis0Args<T>& a, cudaStream_t st) {
   using K = R4Tile<T, DIM, NL>;
   auto k = &green_axis0_r4_kernel<T, DIM, NL, TAB>;
   static bool attr = false;
@@ -422,36 +581,20 @@ cudaError_t axis0_go(const Axis0Args<T>& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, K::THREADS, K::SMEM) !=
-          cudaSuccess ||
-      per_sm < 1) {
-    cudaGetLastError();
-    per_sm = 1;
-  }
-  if (g_sm_count == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        g_sm_count <= 0)
-      g_sm_count = 148;
-  }
   const int64_t tiles = (a.inner + K::WC - 1) / K::WC * ((a.L + K::LT - 1) / K::LT);
-  const int64_t g = (int64_t)per_sm * g_sm_count;
-  const int grid = (int)(tiles < g ? tiles : g);
-  k<<<grid, K::THREADS, K::SMEM, st>>>(a);
+  k<<<persistent_grid(k, K::THREADS, K::SMEM, tiles), K::THREADS, K::SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
 template <typename T, int DIM, bool TAB>
 cudaError_t axis0_n(const Axis0Args<T>& a, int n0, cudaStream_t st) {
   switch (n0) {
-    case 32: return axis0_go<T, DIM, 8, TAB>(a, st);
-    case 64: return axis0_go<T, DIM, 16, TAB>(a, st);
-    case 128: return axis0_go<T, DIM, 32, TAB>(a, st);
-    case 256: return axis0_go<T, DIM, 64, TAB>(a, st);
-    case 512: return axis0_go<T, DIM, 128, TAB>(a, st);
-    default: return axis0_go<T, DIM, 256, TAB>(a, st);
+    case 32: return axis0_r8_go<T, DIM, 32, TAB>(a, st);
+    case 64: return axis0_r8_go<T, DIM, 64, TAB>(a, st);
+    case 128: return axis0_r8_go<T, DIM, 128, TAB>(a, st);
+    case 256: return axis0_r8_go<T, DIM, 256, TAB>(a, st);
+    case 512: return axis0_r4_go<T, DIM, 128, TAB>(a, st);
+    default: return axis0_r4_go<T, DIM, 256, TAB>(a, st);
   }
 }
 

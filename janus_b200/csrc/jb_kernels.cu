@@ -1764,8 +1764,8 @@ cudaError_t fetch_fault_async(unsigned* host, cudaStream_t st) {
                                    cudaMemcpyDeviceToHost, st);
 }
 
-cudaError_t set_first_wait_limit(unsigned polls) {
-  const unsigned v = polls ? polls : kWaitLimit;
+cudaError_t set_first_wait_limit(int polls) {
+  const unsigned v = polls < 0 ? kWaitLimit : (unsigned)polls;
   return cudaMemcpyToSymbol(c_jb_wait_first, &v, sizeof(unsigned));
 }
 

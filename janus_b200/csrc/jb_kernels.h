@@ -111,7 +111,7 @@ cudaError_t read_and_clear_fault(unsigned* out);
 // queue a copy of the fault word to `host` on `st` (read after a stream sync)
 cudaError_t fetch_fault_async(unsigned* host, cudaStream_t st);
 // polls of the first bounded wait of every copy (0: the default limit)
-cudaError_t set_first_wait_limit(unsigned polls);
+cudaError_t set_first_wait_limit(int polls);  // negative: the default
 
 // Spectral row pitch (complex elements) of the solver's internal half
 // spectrum: m * C, plus one where FP32 rows of m * C complex would not span a

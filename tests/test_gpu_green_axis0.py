@@ -1,8 +1,9 @@
-"""The axis-0 Green pass whose middle radix-4 stage and contraction run in
-registers (n0 = 32 ... 1024), against the oracle and against the
-shared-memory column kernel, for the three discretisations of
-janus/green.pyx (truncated 393-580, filtered 583-973 through the generic
-c_apply 185-216 / 356-390, finite differences 976-1036).
+"""The axis-0 Green pass whose transforms and contraction run in registers
+(five-phase tiles for n0 = 32 ... 256, lane-split tiles for 512 and 1024),
+against the oracle and against the shared-memory column kernel, for the
+three discretisations of janus/green.pyx (truncated 393-580, filtered
+583-973 through the generic c_apply 185-216 / 356-390, finite differences
+976-1036).
 
 Shapes are chosen so that the last tile of the pass is ragged (coefficient
 counts that do not fill the last tile, odd load-case counts), which the
@@ -19,11 +20,11 @@ from oracle import janus_oracle as O
 MU = 0.75
 NU = 0.3
 FACTORY = {"truncated": truncated, "filtered": filtered, "willot": willot2015}
-# n0 from 32 to 1024 (one lane per column slice up to 64, split over 2 to 16
-# lanes above); ragged coefficient counts in the last tile
+# n0 from 32 to 1024 (five-phase tiles up to 256, lanes split 8 and 16 ways
+# above); ragged coefficient counts in the last tile
 SHAPES = [(128, 6, 10), (64, 5, 8), (32, 9, 6), (256, 3, 6), (512, 2, 4), (1024, 1, 6),
           (128, 18), (64, 7), (32, 33), (256, 10), (512, 6), (1024, 14)]
-# register radix-4 Green pass (compile-time value 3), the contraction by the
+# register-tile Green pass (compile-time value 3), the contraction by the
 # built-in rule
 R4 = [0, 0, 1, 0, 0, 3, 0]
 
