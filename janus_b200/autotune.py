@@ -7,8 +7,8 @@ n = 64, 128, 256; runtime mixed-radix plans otherwise); what is tuned is how
 the column passes tile the spectrum: the width of a tile in complex columns,
 how many input tiles rotate through shared memory, whether the compile-time
 tiles are used (for the Green pass also in place, without a partner tile,
-24 columns wide at n = 128 and 12 at n = 256, or the pass whose middle
-radix-4 stage and contraction run in registers, n0 = 32, 64, 128), and
+24 columns wide at n = 128 and 12 at n = 256, or the pass whose transforms
+and contraction run in registers, n0 = 32 ... 1024), and
 whether the Green contraction reads the per-coefficient table of symmetric
 Mandel matrices or evaluates the operator on the fly.  Each candidate is timed on the solver step it
 will serve (CUDA events around every pass, several steps after a warm-up),
@@ -57,8 +57,8 @@ def candidates(dim, dtype):
                                                                           (2 * s, 2, 0)]
     # tiles transformed in place: 24 columns at n = 128, 12 at n = 256 (other
     # lengths run these as ordinary compile-time or runtime-plan tiles); the
-    # pass with its middle radix-4 stage in registers (n0 = 32, 64, 128; its
-    # tile is fixed; other lengths run the compile-time tiles)
+    # pass whose transforms run in registers (n0 = 32 ... 1024; its tile is
+    # fixed; other lengths run the compile-time tiles)
     green += [(24, 2, 2), (12, 2, 2), (0, 0, 3)]
     return (plain if dim == 3 else []), green
 

@@ -1680,10 +1680,14 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     // at n = 128 (measured on B200, 128^3 x 6 and 256^3 x 2: Green pass FP64
     // 256: -17%, FP32 256: -8%, FP32 128: -5%, FP64 128: equal)
     const bool rule = !tune || (tune->w == 0 && tune->nbuf == 0 && tune->ct == 1);
-    // the register radix-4 Green pass (n = 32, 64, 128): tuning value ct = 3,
-    // and the built-in rule wherever it exists
+    // the register-tile Green pass (n = 32 ... 1024): tuning value ct = 3;
+    // the built-in rule takes it except where the in-place tiles measured
+    // faster on B200 (3D n = 256: 1.22 vs 1.41 ms FP64 at 256^3 x 2; FP32 on
+    // the fly at 3D n = 128: 0.191 vs 0.210 ms at 128^3 x 6)
+    const bool rule_reg = rule && !(dim == 3 && n == 256) &&
+                          !(dim == 3 && n == 128 && sizeof(T) == 4 && a.mn == nullptr);
     if (mode == 2 && gt && green_axis0_r4_supported(n, C, dim) &&
-        ((tune && tune->ct == 3) || rule)) {
+        ((tune && tune->ct == 3) || rule_reg)) {
       GreenDeviceTables g2 = *gt;
       g2.mn = a.mn;
       const cudaError_t e = launch_green_axis0_r4(sizeof(T) == 8 ? F64 : F32, ax, outer, inner,
