@@ -30,14 +30,11 @@
 // 85 registers (128 where both transforms hold 16 values), so that three
 // CTAs of 256 threads share an SM.
 //
-// n0 = 512, 1024: lane-split tiles.  n0 = 4 NL, n = j + 4 m, k = k1 + NL k2;
-// phase 1: the S = NL/16 lanes of a (column, j) slice each load 16 values
-// (m = a + S b), transform them in registers, apply w_NL^(a e) and finish
-// the NL-point transform across the S lanes by shuffles (radix-2 steps and a
-// bit-reversal exchange); phase 2: one lane per (k1, group) applies the
-// twiddles w_n0^(j k1), the 4-point transform over j, the contraction at the
-// four rows b0 = k1 + NL k2, and the inverse; phase 3 mirrors phase 1.  The
-// next tile's rows are prefetched into L2 while a tile is transformed.
+// n0 = 512, 1024: seven-phase tiles, the same scheme with the N2-point
+// transform split once more (512 = 8 8 8, 1024 = 16 8 8): P1, then an
+// 8-point transform over the high part of j with its twiddles, an 8-point
+// transform over the low part, the contraction, and the mirror images; the
+// middle phases loop over more jobs than the block has lanes.
 //
 // No waits besides the block barriers.
 #include <cuda_runtime.h>
@@ -49,7 +46,7 @@
 namespace jb {
 namespace {
 
-// ---- shared by both tile kinds ----
+// ---- shared by the tile kinds ----
 
 template <typename T> struct Axis0Args {
   const cx<T>* in;
@@ -60,7 +57,6 @@ template <typename T> struct Axis0Args {
   int64_t ncoef;     // F
   int64_t m_last;    // 3D: coefficient f = b1 * m_last + b2
   int L;
-  int prefetch;      // rows 16-byte aligned (lane-split tiles: L2 prefetch)
   GreenTables<T> gt;
   const T* tab;      // symmetric Mandel matrices [f][c][b0], or nullptr: on the fly
 };
@@ -326,254 +322,167 @@ cudaError_t axis0_r8_go(const Axis0Args<T>& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// ---- lane-split tiles (n0 = 512, 1024) ----
+// ---- seven-phase tiles (n0 = 512, 1024) ----
 
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
+// n0 = N1 A B: n = j + M m (M = A B), k = k1 + N1 k2; the M-point transform
+// over j = ja + A jb is split again, k2 = kb + B ka:
+//   sum_j w_M^(j k2) z_j = sum_ja w_A^(ja ka) [w_M^(ja kb) sum_jb w_B^(jb kb) z_(ja + A jb)].
+// A tile is one load case x 6 columns x n0 rows in shared memory as
+// S[k1][p][c] (p = ja + A jb, then ja + A kb, then ka + A kb).  P1 (lane per
+// column and j): N1-point transform over m and the twiddles w_n0^(j k1);
+// 2a (job per k1, ja, column): B-point transform over jb and the twiddles
+// w_M^(ja kb); 2a' (job per k1, kb, column): A-point transform over ja; 2b
+// (job per k1, kb, ka): the contraction at b0 = k1 + N1 (kb + B ka); then
+// the mirror images.  The middle phases have more jobs than the block has
+// lanes and loop over them.  k1 stride padded by one value: every phase is
+// free of bank conflicts in FP64 (searched on the CPU, like the five-phase
+// tiles).
+template <int N0> struct R16Shape;
+template <> struct R16Shape<512> { static constexpr int N1 = 8, A = 8, B = 8; };
+template <> struct R16Shape<1024> { static constexpr int N1 = 16, A = 8, B = 8; };
 
-// lanes per column slice of the lane-split tiles: NL = 16 S is split over S
-// consecutive lanes of a warp, 16 values each, m = a + S b for lane a
-template <int NL> struct LaneSplit {
-  static_assert(NL >= 64 && NL % 16 == 0, "lane-split tiles: NL = 16 S, S >= 4");
-  static constexpr int SPL = NL / 16;
-  static constexpr int V = 16;
-};
-
-// row (relative to j) of value i of lane a (n = j + 4 m)
-template <int NL> __device__ __forceinline__ int lane_row(int i, int a) {
-  return 4 * (a + LaneSplit<NL>::SPL * i);
-}
-
-template <int S> __device__ __forceinline__ int bit_reverse(int x) {
-  int r = 0;
-#pragma unroll
-  for (int m = 1; m < S; m <<= 1) {
-    r = (r << 1) | (x & 1);
-    x >>= 1;
-  }
-  return r;
-}
-
-// S-point DFT across the S lanes of a slice (S = 4, 8, 16) for each of the
-// 16 values: lane a holds V_a[e]; on return lane d holds
-// sum_a w_S^(DIR a d) V_a[e].  Radix-2 decimation in frequency over the lane
-// index (the lower lane of a pair keeps u + o, the upper (o - u) w_2h^q,
-// q = a mod h, both as fma(sg, u, o) times a twiddle that is exactly 1 on the
-// lower lane), then a bit-reversal permutation of the lanes.  tw: the axis
-// table exp(-2 pi i t / n0), n0 = 64 S.
-template <int S, int DIR, typename C>
-__device__ __forceinline__ void cross_lane_dft(C* v, int a, const C* tw) {
-  using T = decltype(v[0].x);
-  constexpr int N0 = 64 * S;
-#pragma unroll
-  for (int h = S / 2; h >= 1; h >>= 1) {
-    const bool upper = (a & h) != 0;
-    asm volatile("" ::: "memory");  // one stage's twiddle live at a time
-    const C wt = tw[(a % h) * (N0 / (2 * h))];
-    const C w = upper ? (DIR > 0 ? cconj(wt) : wt) : mkc(T(1), T(0));
-    const T sg = upper ? T(-1) : T(1);
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      const C u = v[e];
-      const C o = mkc(__shfl_xor_sync(0xffffffffu, u.x, h), __shfl_xor_sync(0xffffffffu, u.y, h));
-      v[e] = cmul(mkc(fma(sg, u.x, o.x), fma(sg, u.y, o.y)), w);
-    }
-  }
-  const int src = ((threadIdx.x & 31) & ~(S - 1)) | bit_reverse<S>(a);
-#pragma unroll
-  for (int e = 0; e < 16; ++e)
-    v[e] = mkc(__shfl_sync(0xffffffffu, v[e].x, src), __shfl_sync(0xffffffffu, v[e].y, src));
-}
-
-// forward transform over m of a column slice: on entry v[i] holds row
-// j + 4 m(i, a); on return v[i] = Y[k1] at k1 = i + 16 a
-template <int NL, typename C>
-__device__ __forceinline__ void lane_fwd(C* v, int a, const C* tw) {
-  constexpr int S = LaneSplit<NL>::SPL;
-  Dft<16, -1, C>::run(v);
-  // V_a[e] = w_NL^(a e) U_a[e], w_NL = w_n0^4; the twiddles are read here,
-  // not ahead of the transform, where they would only hold registers
-  asm volatile("" ::: "memory");
-#pragma unroll
-  for (int e = 1; e < 16; ++e) v[e] = cmul(v[e], tw[4 * a * e]);
-  cross_lane_dft<S, -1>(v, a, tw);
-}
-
-// inverse: v[i] = V[k1] at k1 = i + 16 a -> v[i] = x at row j + 4 m(i, a)
-template <int NL, typename C>
-__device__ __forceinline__ void lane_inv(C* v, int a, const C* tw) {
-  constexpr int S = LaneSplit<NL>::SPL;
-  cross_lane_dft<S, +1>(v, a, tw);
-  asm volatile("" ::: "memory");
-#pragma unroll
-  for (int e = 1; e < 16; ++e) v[e] = cmulc(v[e], tw[4 * a * e]);
-  Dft<16, +1, C>::run(v);
-}
-
-// lane-split tile geometry for n0 = 4 NL (one load case, one 6-column group)
-template <typename T, int DIM, int NL> struct R4Tile {
+template <typename T, int DIM, int N0> struct R16Tile {
+  static constexpr int N1 = R16Shape<N0>::N1, A = R16Shape<N0>::A, B = R16Shape<N0>::B;
+  static constexpr int M = A * B;
   static constexpr int C = DIM == 3 ? 6 : 3;
-  static constexpr int LT = 1;                    // load cases per tile
-  static constexpr int NG = 1;                    // 6-column groups per tile
-  static constexpr int WC = 6 * NG;               // columns per tile
-  static constexpr int SPL = LaneSplit<NL>::SPL;
-  static constexpr int P1 = LT * WC * 4 * SPL;    // phase-1/3 threads
-  static constexpr int P2 = LT * NL * NG;         // phase-2 threads
-  static constexpr int THREADS = P1 > P2 ? P1 : P2;
-  static constexpr int P = 4 * WC + 1;            // k1 stride (odd)
-  // shared-memory phases: 8 lanes of 16 bytes (FP64), 16 of 8 bytes (FP32)
-  static constexpr int LMOD = sizeof(T) == 8 ? 8 : 16;
-  // block d of 16 values (lane d of a split slice) sits d OSTEP further on,
-  // so that the lanes of a slice write disjoint banks
-  static constexpr int OSTEP = SPL >= LMOD ? 1 : LMOD / SPL;
-  static constexpr int LS = NL * P + SPL * OSTEP;
-  static constexpr size_t SMEM = (size_t)LT * LS * sizeof(cx<T>);
-  // resident CTAs asked of the register allocator
-  static constexpr int MINB = THREADS > 256 ? 1 : (sizeof(T) == 8 ? 2 : 3);
+  static constexpr int WC = 6;
+  static constexpr int THREADS = WC * M;  // P1 lanes (c, j)
+  static constexpr int J2A = N1 * A * WC;
+  static constexpr int J2A_ = N1 * B * WC;
+  static constexpr int J2B = N1 * M;
+  static constexpr int PJ = WC;
+  static constexpr int PK = M * PJ + 1;
+  static constexpr size_t SMEM = (size_t)N1 * PK * sizeof(cx<T>);
+  // 24 warps per SM in FP64 (at most 85 registers), 32 in FP32
+  static constexpr int MINB = (sizeof(T) == 8 ? 24 : 32) * 32 / THREADS;
 };
 
-// offset of value k1 in a (load case, j, column) slice
-template <typename K> __device__ __forceinline__ int k1_off(int k1) {
-  return k1 * K::P + (k1 >> 4) * K::OSTEP;
-}
-
-template <typename T, int DIM, int NL, bool TAB>
-__global__ void __launch_bounds__(R4Tile<T, DIM, NL>::THREADS, R4Tile<T, DIM, NL>::MINB)
-    green_axis0_r4_kernel(Axis0Args<T> a) {
+template <typename T, int DIM, int N0, bool TAB>
+__global__ void __launch_bounds__(R16Tile<T, DIM, N0>::THREADS, R16Tile<T, DIM, N0>::MINB)
+    green_axis0_r16_kernel(Axis0Args<T> a) {
   using C = cx<T>;
-  using K = R4Tile<T, DIM, NL>;
-  constexpr int N0 = 4 * NL;
-  constexpr int NV = LaneSplit<NL>::V;  // 16
+  using K = R16Tile<T, DIM, N0>;
+  constexpr int N1 = K::N1, A = K::A, B = K::B, M = K::M;
+  constexpr int TS = N0 / M;  // w_M = w_n0^TS
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* S = reinterpret_cast<C*>(smem_raw);
   const int tid = threadIdx.x;
-  // phase-1/3 lane: lane a1 of a split slice, column c, load case l1, j1
-  const bool p1 = tid < K::P1;
-  const int a1 = tid % K::SPL;
-  const int s1 = tid / K::SPL;
-  const int c = s1 % K::WC;
-  const int l1 = (s1 / K::WC) % K::LT;
-  const int j1 = s1 / (K::WC * K::LT);
-  // phase-2 lane: load case l2, k1, group g2
-  const bool p2 = tid < K::P2;
-  const int l2 = tid % K::LT;
-  const int k1 = (tid / K::LT) % NL;
-  const int g2 = tid / (K::LT * NL);
-  const int64_t nchunk = (a.inner + K::WC - 1) / K::WC;
-  const int LP = (a.L + K::LT - 1) / K::LT;
-  const int64_t total = nchunk * LP;
-  const int64_t lstride = (int64_t)N0 * a.pitch;
+  const int LP = a.L;
+  const int64_t total = (a.inner + K::WC - 1) / K::WC * LP;
   for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
     const int64_t chunk = t / LP;
-    const int lp = (int)(t - chunk * LP);
+    const int lg = (int)(t - chunk * LP);
     const int64_t col0 = chunk * K::WC;
-    // the next tile's rows head for L2 while this one is transformed
-    if (a.prefetch) {
-      const int64_t tn = t + gridDim.x;
-      if (tn < total) {
-        const int64_t cn = tn / LP;
-        const int lpn = (int)(tn - cn * LP);
-        const int64_t cols = min((int64_t)K::WC, a.inner - cn * K::WC);
-        const uint32_t bytes = (uint32_t)(cols * sizeof(C)) & ~15u;
-        for (int q = tid; q < K::LT * N0; q += blockDim.x) {
-          const int l = lpn * K::LT + q / N0;
-          if (l < a.L && bytes > 0)
-            prefetch_l2(a.in + l * lstride + (int64_t)(q % N0) * a.pitch + cn * K::WC, bytes);
-        }
-      }
-    }
-    // phase 1: load the slice's rows, transform over m.  The row pitch is
-    // re-read opaquely each tile so that the row offsets are not hoisted out
-    // of the tile loop (they would stay live through phase 2)
-    int64_t pitch;
-    asm volatile("mov.b64 %0, %1;" : "=l"(pitch) : "l"(a.pitch));
-    C v[NV];
-    const int64_t col = col0 + c;
-    const int lg1 = lp * K::LT + l1;
-    const bool ok1 = p1 && col < a.inner && lg1 < a.L;
-    if (p1) {
-      const C* src = a.in + lg1 * lstride + (int64_t)j1 * pitch + col;
+    // P1: lane (c, j): N1-point transform over m, twiddles w_n0^(j k1)
+    {
+      const int tq = opaque(tid);
+      const int c = tq % K::WC, j = tq / K::WC;
+      const bool ok = col0 + c < a.inner;
+      C v[N1];
+      const int64_t pitch = a.pitch;
+      const C* src = a.in + ((int64_t)lg * N0 + j) * pitch + col0 + c;
 #pragma unroll
-      for (int i = 0; i < NV; ++i)
-        v[i] = ok1 ? src[(int64_t)lane_row<NL>(i, a1) * pitch] : mkc(T(0), T(0));
-      lane_fwd<NL>(v, a1, a.tw);
-    }
-    // (no barrier: phase 3 of the previous tile read these positions in
-    // this same lane)
-    if (p1) {
-      C* s = S + l1 * K::LS + j1 * K::WC + c;
+      for (int m = 0; m < N1; ++m) v[m] = ok ? src[(int64_t)m * M * pitch] : mkc(T(0), T(0));
+      Dft<N1, -1, C>::run(v);
+      asm volatile("" ::: "memory");
 #pragma unroll
-      for (int i = 0; i < NV; ++i) s[k1_off<K>(i + NV * a1)] = v[i];
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], a.tw[j * k1]);
+      C* s = S + j * K::PJ + c;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) s[k1 * K::PK] = v[k1];
     }
     __syncthreads();
-    // phase 2: twiddles, 4-point transform, Green contraction, and back
-    const int lg2 = lp * K::LT + l2;
-    if (p2 && lg2 < a.L) {
-      C* s = S + l2 * K::LS + k1_off<K>(k1) + g2 * 6;
-      C x[4][6];
+    // 2a: job (k1, ja, c): B-point transform over jb, twiddles w_M^(ja kb)
+    for (int job = opaque(tid); job < K::J2A; job += K::THREADS) {
+      const int k1 = job % N1, ja = (job / N1) % A, c = job / (N1 * A);
+      C* s = S + k1 * K::PK + ja * K::PJ + c;
+      C w[B];
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int jb = 0; jb < B; ++jb) w[jb] = s[A * jb * K::PJ];
+      Dft<B, -1, C>::run(w);
+      asm volatile("" ::: "memory");
 #pragma unroll
-        for (int q = 0; q < 6; ++q) x[j][q] = s[j * K::WC + q];
-      // w_n0^(j k1), j = 1..3 (read each tile: nothing stays live across phases)
-      const C tw1 = a.tw[k1], tw2 = a.tw[2 * k1], tw3 = a.tw[3 * k1];
+      for (int kb = 1; kb < B; ++kb) w[kb] = cmul(w[kb], a.tw[TS * ja * kb]);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        C g4[4] = {x[0][q], cmul(x[1][q], tw1), cmul(x[2][q], tw2), cmul(x[3][q], tw3)};
-        Dft<4, -1, C>::run(g4);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) x[k][q] = g4[k];
-      }
-      // coefficients of the group (3D: one; 2D: two of three components)
-      const int64_t fbase = (col0 + g2 * 6) / K::C;
-#pragma unroll
-      for (int k2 = 0; k2 < 4; ++k2) {
-        const int b0 = k1 + NL * k2;
-#pragma unroll
-        for (int h = 0; h < 6 / K::C; ++h) {
-          const int64_t f = fbase + h;
-          if (f < a.ncoef) contract<T, DIM, TAB>(a, f, b0, N0, &x[k2][h * K::C]);
-        }
-        // one row's operator values live at a time
-        asm volatile("" ::: "memory");
-      }
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        C g4[4] = {x[0][q], x[1][q], x[2][q], x[3][q]};
-        Dft<4, +1, C>::run(g4);
-        x[0][q] = g4[0];
-        x[1][q] = cmulc(g4[1], tw1);
-        x[2][q] = cmulc(g4[2], tw2);
-        x[3][q] = cmulc(g4[3], tw3);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) s[j * K::WC + q] = x[j][q];
+      for (int kb = 0; kb < B; ++kb) s[A * kb * K::PJ] = w[kb];
     }
     __syncthreads();
-    // phase 3: read the slice back, inverse transform over k1, store
-    if (p1) {
-      const C* s = S + l1 * K::LS + j1 * K::WC + c;
+    // 2a': job (k1, kb, c): A-point transform over ja
+    for (int job = opaque(tid); job < K::J2A_; job += K::THREADS) {
+      const int k1 = job % N1, kb = (job / N1) % B, c = job / (N1 * B);
+      C* s = S + k1 * K::PK + A * kb * K::PJ + c;
+      C w[A];
 #pragma unroll
-      for (int i = 0; i < NV; ++i) v[i] = s[k1_off<K>(i + NV * a1)];
-      lane_inv<NL>(v, a1, a.tw);
-      if (ok1) {
-        int64_t pitch3;
-        asm volatile("mov.b64 %0, %1;" : "=l"(pitch3) : "l"(a.pitch));
-        C* dst = a.out + lg1 * lstride + (int64_t)j1 * pitch3 + col;
+      for (int ja = 0; ja < A; ++ja) w[ja] = s[ja * K::PJ];
+      Dft<A, -1, C>::run(w);
 #pragma unroll
-        for (int i = 0; i < NV; ++i) __stcs(dst + (int64_t)lane_row<NL>(i, a1) * pitch3, v[i]);
+      for (int ka = 0; ka < A; ++ka) s[ka * K::PJ] = w[ka];
+    }
+    __syncthreads();
+    // 2b: job (k1, kb, ka): the contraction at b0 = k1 + N1 (kb + B ka)
+    for (int job = opaque(tid); job < K::J2B; job += K::THREADS) {
+      const int k1 = job % N1, kb = (job / N1) % B, ka = job / (N1 * B);
+      C* s = S + k1 * K::PK + (ka + A * kb) * K::PJ;
+      C y[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) y[q] = s[q];
+      contract_row<T, DIM, TAB>(a, col0 / K::C, k1 + N1 * (kb + B * ka), N0, y, s);
+    }
+    __syncthreads();
+    // 2c': inverse over ka
+    for (int job = opaque(tid); job < K::J2A_; job += K::THREADS) {
+      const int k1 = job % N1, kb = (job / N1) % B, c = job / (N1 * B);
+      C* s = S + k1 * K::PK + A * kb * K::PJ + c;
+      C w[A];
+#pragma unroll
+      for (int ja = 0; ja < A; ++ja) w[ja] = s[ja * K::PJ];
+      Dft<A, +1, C>::run(w);
+#pragma unroll
+      for (int ja = 0; ja < A; ++ja) s[ja * K::PJ] = w[ja];
+    }
+    __syncthreads();
+    // 2c: conjugate twiddles, inverse over kb
+    for (int job = opaque(tid); job < K::J2A; job += K::THREADS) {
+      const int k1 = job % N1, ja = (job / N1) % A, c = job / (N1 * A);
+      C* s = S + k1 * K::PK + ja * K::PJ + c;
+      C w[B];
+#pragma unroll
+      for (int kb = 0; kb < B; ++kb) w[kb] = s[A * kb * K::PJ];
+      asm volatile("" ::: "memory");
+#pragma unroll
+      for (int kb = 1; kb < B; ++kb) w[kb] = cmulc(w[kb], a.tw[TS * ja * kb]);
+      Dft<B, +1, C>::run(w);
+#pragma unroll
+      for (int jb = 0; jb < B; ++jb) s[A * jb * K::PJ] = w[jb];
+    }
+    __syncthreads();
+    // P3: conjugate twiddles, inverse over k1, store (no barrier before the
+    // next tile's P1: it writes only the positions this lane reads here)
+    {
+      const int tq = opaque(tid);
+      const int c = tq % K::WC, j = tq / K::WC;
+      C v[N1];
+      const C* s = S + j * K::PJ + c;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) v[k1] = s[k1 * K::PK];
+      asm volatile("" ::: "memory");
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulc(v[k1], a.tw[j * k1]);
+      Dft<N1, +1, C>::run(v);
+      if (col0 + c < a.inner) {
+        const int64_t pitch = a.pitch;
+        C* dst = a.out + ((int64_t)lg * N0 + j) * pitch + col0 + c;
+#pragma unroll
+        for (int m = 0; m < N1; ++m) __stcs(dst + (int64_t)m * M * pitch, v[m]);
       }
     }
   }
 }
 
-template <typename T, int DIM, int NL, bool TAB>
-cudaError_t axis0_r4_go(const Axis0Args<T>& a, cudaStream_t st) {
-  using K = R4Tile<T, DIM, NL>;
-  auto k = &green_axis0_r4_kernel<T, DIM, NL, TAB>;
+template <typename T, int DIM, int N0, bool TAB>
+cudaError_t axis0_r16_go(const Axis0Args<T>& a, cudaStream_t st) {
+  using K = R16Tile<T, DIM, N0>;
+  auto k = &green_axis0_r16_kernel<T, DIM, N0, TAB>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -581,7 +490,7 @@ cudaError_t axis0_r4_go(const Axis0Args<T>& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int64_t tiles = (a.inner + K::WC - 1) / K::WC * ((a.L + K::LT - 1) / K::LT);
+  const int64_t tiles = (a.inner + K::WC - 1) / K::WC * a.L;
   k<<<persistent_grid(k, K::THREADS, K::SMEM, tiles), K::THREADS, K::SMEM, st>>>(a);
   return cudaGetLastError();
 }
@@ -593,8 +502,8 @@ cudaError_t axis0_n(const Axis0Args<T>& a, int n0, cudaStream_t st) {
     case 64: return axis0_r8_go<T, DIM, 64, TAB>(a, st);
     case 128: return axis0_r8_go<T, DIM, 128, TAB>(a, st);
     case 256: return axis0_r8_go<T, DIM, 256, TAB>(a, st);
-    case 512: return axis0_r4_go<T, DIM, 128, TAB>(a, st);
-    default: return axis0_r4_go<T, DIM, 256, TAB>(a, st);
+    case 512: return axis0_r16_go<T, DIM, 512, TAB>(a, st);
+    default: return axis0_r16_go<T, DIM, 1024, TAB>(a, st);
   }
 }
 
@@ -623,7 +532,6 @@ cudaError_t axis0_t(const AxisData& ax0, int64_t L, int64_t inner, int64_t pitch
   a.ncoef = inner / C;
   a.m_last = m_last;
   a.L = (int)L;
-  a.prefetch = al(in, 16) && (pitch * cs) % 16 == 0;
   GreenTables<T> t{};
   for (int d = 0; d < 3; ++d) {
     t.kt[d] = static_cast<const T*>(gt.kt[d]);
