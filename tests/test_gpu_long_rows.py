@@ -1,5 +1,6 @@
-"""Row passes along 512- and 1024-point axes (the register FFT of the long
-axes): the FFT objects against numpy's FFT with the reference's tolerance
+"""Row passes along 512- and 1024-point axes (one or two rows per CTA of the
+runtime-plan row kernels): the FFT objects against numpy's FFT with the
+reference's tolerance
 model (tests/test_fft.py:9-80 of the reference), and the basic scheme on
 grids whose rows are that long against the oracle, per iterate
 (janus/fft/serial/_serial_fft.pyx:152-163 r2c, 177-190 c2r; the scheme of
