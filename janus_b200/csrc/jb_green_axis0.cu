@@ -206,7 +206,7 @@ template <typename T, int DIM, int N0> struct R8Tile {
   static constexpr int THREADS = P1 > P2A ? (P1 > P2B ? P1 : P2B) : (P2A > P2B ? P2A : P2B);
   static constexpr int PJ = WC;
   static constexpr int PK = N2 * PJ + (sizeof(T) == 8 || NG != 2 ? 1 : 2);
-  static constexpr size_t SMEM = (size_t)N1 * PK * sizeof(cx<T>);
+  static constexpr size_t SMEM = ((size_t)N1 * PK + N0) * sizeof(cx<T>);
   // resident CTAs asked of the register allocator: 24 warps per SM in FP64
   // (at most 85 registers; 16 warps and 128 registers where both transform
   // phases hold 16 values), 40 in FP32 (51 registers; 32 where both hold 16).
@@ -225,7 +225,13 @@ __global__ void __launch_bounds__(R8Tile<T, DIM, N0>::THREADS, R8Tile<T, DIM, N0
   constexpr int N1 = K::N1, N2 = K::N2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* S = reinterpret_cast<C*>(smem_raw);
+  // the axis twiddles, copied once per CTA: P1 and P3 read them from shared
+  // memory (measured 0.364 -> 0.352 ms FP64, 0.196 -> 0.191 ms FP32 against
+  // reading them through L1 at 128^3 x 6)
+  C* TW = S + (size_t)N1 * K::PK;
   const int tid = threadIdx.x;
+  for (int i = tid; i < N0; i += blockDim.x) TW[i] = a.tw[i];
+  __syncthreads();
   const int LP = a.L;
   const int64_t total = (a.inner + K::WC - 1) / K::WC * LP;
   for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
@@ -245,7 +251,7 @@ __global__ void __launch_bounds__(R8Tile<T, DIM, N0>::THREADS, R8Tile<T, DIM, N0
       Dft<N1, -1, C>::run(v);
       asm volatile("" ::: "memory");
 #pragma unroll
-      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], a.tw[j * k1]);
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], TW[j * k1]);
       C* s = S + j * K::PJ + c;
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) s[k1 * K::PK] = v[k1];
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(R8Tile<T, DIM, N0>::THREADS, R8Tile<T, DIM, N0
       for (int k1 = 0; k1 < N1; ++k1) v[k1] = s[k1 * K::PK];
       asm volatile("" ::: "memory");
 #pragma unroll
-      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulc(v[k1], a.tw[j * k1]);
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulc(v[k1], TW[j * k1]);
       Dft<N1, +1, C>::run(v);
       if (col0 + c < a.inner) {
         const int64_t pitch = a.pitch;
