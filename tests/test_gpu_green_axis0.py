@@ -22,8 +22,8 @@ NU = 0.3
 FACTORY = {"truncated": truncated, "filtered": filtered, "willot": willot2015}
 # n0 from 32 to 1024 (five-phase tiles up to 256, seven-phase above); ragged
 # coefficient counts in the last tile
-SHAPES = [(128, 6, 10), (64, 5, 8), (32, 9, 6), (256, 3, 6), (512, 2, 4), (1024, 1, 6),
-          (128, 18), (64, 7), (32, 33), (256, 10), (512, 6), (1024, 14)]
+SHAPES = [(128, 6, 10), (128, 5, 4), (64, 5, 8), (32, 9, 6), (256, 3, 6), (512, 2, 4),
+          (1024, 1, 6), (128, 18), (64, 7), (32, 33), (256, 10), (512, 6), (1024, 14)]
 # register-tile Green pass (compile-time value 3), the contraction by the
 # built-in rule
 R4 = [0, 0, 1, 0, 0, 3, 0]
