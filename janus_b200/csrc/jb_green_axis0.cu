@@ -70,47 +70,38 @@ __device__ __forceinline__ int opaque(int x) {
   return r;
 }
 
-// the Green contraction of coefficient f at row b0 (te: its C components):
-// through the table (TAB), or on the fly for the single-alias operators
-// (truncated, finite differences)
-template <typename T, int DIM, bool TAB>
-__device__ __forceinline__ void contract(const Axis0Args<T>& a, int64_t f, int b0, int n0,
-                                         cx<T>* te) {
-  if constexpr (TAB) {
-    constexpr int NT = GSize<DIM>::value;
-    const T* g = a.tab + (size_t)f * NT * n0 + b0;
-    T gv[NT];
-#pragma unroll
-    for (int c = 0; c < NT; ++c) gv[c] = __ldg(g + (size_t)c * n0);
-    g_apply<DIM, T>(gv, te);
+// the Green contraction of coefficient f at row b0 on the fly (te: its C
+// components), for the single-alias operators (truncated, finite
+// differences); the table form is in contract_row
+template <typename T, int DIM>
+__device__ __forceinline__ void contract_fly(const Axis0Args<T>& a, int64_t f, int b0,
+                                             cx<T>* te) {
+  constexpr int S = DIM == 3 ? 6 : 3;
+  int b1, b2;
+  if (DIM == 3) {
+    b1 = (int)(f / a.m_last);
+    b2 = (int)(f - (int64_t)b1 * a.m_last);
   } else {
-    constexpr int S = DIM == 3 ? 6 : 3;
-    int b1, b2;
-    if (DIM == 3) {
-      b1 = (int)(f / a.m_last);
-      b2 = (int)(f - (int64_t)b1 * a.m_last);
-    } else {
-      b1 = (int)f;
-      b2 = 0;
-    }
-    const AxisK<T> a0 = axis_values(a.gt, 0, b0);
-    const AxisK<T> a1 = axis_values(a.gt, 1, b1);
-    const AxisK<T> a2 = DIM == 3 ? axis_values(a.gt, 2, b2) : a1;
-    T k0 = a0.v[0], k1 = a1.v[0], k2 = a2.v[0];
-    if (a.gt.variant == 2) willot_k<DIM, T>(a0.v, a1.v, a2.v, k0, k1, k2);
-    cx<T> t[S], acc[S];
-#pragma unroll
-    for (int i = 0; i < S; ++i) {
-      t[i] = te[i];
-      acc[i] = mkc(T(0), T(0));
-    }
-    if (DIM == 2)
-      gamma2_acc(k0, k1, T(1), t, acc, a.gt.inv2g, a.gt.c1);
-    else
-      gamma3_acc(k0, k1, k2, T(1), t, acc, a.gt.inv2g, a.gt.c1);
-#pragma unroll
-    for (int i = 0; i < S; ++i) te[i] = acc[i];
+    b1 = (int)f;
+    b2 = 0;
   }
+  const AxisK<T> a0 = axis_values(a.gt, 0, b0);
+  const AxisK<T> a1 = axis_values(a.gt, 1, b1);
+  const AxisK<T> a2 = DIM == 3 ? axis_values(a.gt, 2, b2) : a1;
+  T k0 = a0.v[0], k1 = a1.v[0], k2 = a2.v[0];
+  if (a.gt.variant == 2) willot_k<DIM, T>(a0.v, a1.v, a2.v, k0, k1, k2);
+  cx<T> t[S], acc[S];
+#pragma unroll
+  for (int i = 0; i < S; ++i) {
+    t[i] = te[i];
+    acc[i] = mkc(T(0), T(0));
+  }
+  if (DIM == 2)
+    gamma2_acc(k0, k1, T(1), t, acc, a.gt.inv2g, a.gt.c1);
+  else
+    gamma3_acc(k0, k1, k2, T(1), t, acc, a.gt.inv2g, a.gt.c1);
+#pragma unroll
+  for (int i = 0; i < S; ++i) te[i] = acc[i];
 }
 
 // index of entry (i, j) of a symmetric S x S matrix stored as its diagonal
@@ -153,7 +144,7 @@ __device__ __forceinline__ void contract_row(const Axis0Args<T>& a, int64_t fbas
         for (int i = 0; i < S; ++i) dst[h * S + i] = t[i];
       }
     } else {
-      if (f < a.ncoef) contract<T, DIM, false>(a, f, b0, n0, t);
+      if (f < a.ncoef) contract_fly<T, DIM>(a, f, b0, t);
 #pragma unroll
       for (int i = 0; i < S; ++i) dst[h * S + i] = t[i];
     }
@@ -189,7 +180,8 @@ int persistent_grid(KFn k, int threads, size_t smem, int64_t tiles) {
 // (j) stride PJ = 6 NG and k1 stride PK = N2 PJ + pad: the pad (1 for FP64,
 // 2 for FP32 tiles of two groups, 1 otherwise) was found by an exhaustive
 // search of the bank conflicts of every phase's access pattern, all
-// conflict-free except one 2-way phase in FP32.
+// conflict-free except one 2-way phase in FP32.  A copy of the n0 axis
+// twiddles follows the tile.
 template <int N0> struct R8Shape;
 template <> struct R8Shape<32> { static constexpr int N1 = 8, N2 = 4, NG = 4; };
 template <> struct R8Shape<64> { static constexpr int N1 = 8, N2 = 8, NG = 2; };
