@@ -1121,6 +1121,9 @@ __global__ void reduce_rows_kernel(const double* partials, int nb, double* out, 
   }
 }
 
+// long contiguous rows (n = 512, 1024) of 2D fields
+#include "jb_rows_long.cuh"
+
 std::mutex g_attr_mu;
 std::unordered_map<const void*, size_t> g_attr;
 
@@ -1412,6 +1415,72 @@ cudaError_t c2r_ct_dispatch(int C, int epi, const RowsArgs<T>& a, dim3 grid, siz
   return cudaErrorNotSupported;
 }
 
+// Long contiguous rows (n = 512, 1024, three components): the persistent
+// kernels of jb_rows_long.cuh when every row satisfies their bulk-copy rules
+// (16-byte aligned bases and pitches, a spectral row of a multiple of 16
+// bytes, a tail of the spectral row of 3 or 4 complex); cudaErrorNotSupported
+// otherwise, and the general kernels run.
+template <typename T>
+cudaError_t long_r2c_launch(const RowsArgs<T>& a, int n, const LocalDesc* local, cudaStream_t st) {
+  using C = cx<T>;
+  const int ib = local ? local->index_bytes : 0;
+  if (!a.contig || !al16(a.x) || !al16(a.out) || (a.sp * sizeof(C)) % 16 != 0 ||
+      (a.cstride_l * sizeof(C)) % 16 != 0 || (a.g.ls * sizeof(T)) % 16 != 0 ||
+      (ib != 0 && ib != 1 && ib != 4) || (ib != 0 && !al16(local->phase)))
+    return cudaErrorNotSupported;
+  const int tabn = local ? local->nphase * local_entry(local->kind, 2) : 0;
+  const size_t tabb = (local && tabn <= 2 * kTabStage) ? (size_t)tabn * sizeof(T) : 0;
+  const size_t smem = long_r2c_layout(sizeof(C), n, a.sp, (size_t)n * ib, tabb).total;
+  if (smem > kSmemCap - 4096) return cudaErrorNotSupported;
+  const int64_t tiles = a.g.rows * a.L;
+  auto go = [&](auto k, int threads) {
+    cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+    if (e != cudaSuccess) return e;
+    k<<<persistent_grid(k, threads, smem, tiles), threads, smem, st>>>(a);
+    return cudaGetLastError();
+  };
+  constexpr int TH = 192;
+  if (n == 1024) return local ? go(&rows_long_r2c_kernel<T, 1024, true>, TH)
+                              : go(&rows_long_r2c_kernel<T, 1024, false>, TH);
+  return local ? go(&rows_long_r2c_kernel<T, 512, true>, TH)
+               : go(&rows_long_r2c_kernel<T, 512, false>, TH);
+}
+
+template <typename T>
+cudaError_t long_c2r_launch(const RowsArgs<T>& a, int n, int epi, int* nb_out, cudaStream_t st) {
+  using C = cx<T>;
+  const int64_t tail = a.sp - 3 * (int64_t)(n / 2);
+  if (epi == kEpiResid || !a.contig || !al16(a.cin) || !al16(a.y) ||
+      (epi == kEpiRhs && !al16(a.rhs)) || (a.sp * sizeof(C)) % 16 != 0 ||
+      (tail * (int64_t)sizeof(C)) % 16 != 0 || tail < 3 || tail > 4 ||
+      (a.cstride_l * sizeof(C)) % 16 != 0 || (a.g.ls * sizeof(T)) % 16 != 0)
+    return cudaErrorNotSupported;
+  const size_t smem = long_c2r_layout(sizeof(C), n).total;
+  const int64_t tiles = a.g.rows * a.L;
+  auto go = [&](auto k) {
+    cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k), smem);
+    if (e != cudaSuccess) return e;
+    // at most one CTA per row: the partials hold rows slots per load case
+    int grid = persistent_grid(k, 192, smem, tiles);
+    if (grid > a.g.rows) grid = (int)a.g.rows;
+    if (nb_out) *nb_out = grid;
+    k<<<grid, 192, smem, st>>>(a);
+    return cudaGetLastError();
+  };
+  if (n == 1024) {
+    switch (epi) {
+      case kEpiUpdate: return go(&rows_long_c2r_kernel<T, 1024, kEpiUpdate>);
+      case kEpiRhs: return go(&rows_long_c2r_kernel<T, 1024, kEpiRhs>);
+      default: return go(&rows_long_c2r_kernel<T, 1024, kEpiPlain>);
+    }
+  }
+  switch (epi) {
+    case kEpiUpdate: return go(&rows_long_c2r_kernel<T, 512, kEpiUpdate>);
+    case kEpiRhs: return go(&rows_long_c2r_kernel<T, 512, kEpiRhs>);
+    default: return go(&rows_long_c2r_kernel<T, 512, kEpiPlain>);
+  }
+}
+
 template <typename T>
 cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const RealGeom& g,
                        void* out, const LocalDesc* local, cudaStream_t st, int64_t spitch) {
@@ -1449,6 +1518,10 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     a.nphase = local->nphase;
     a.kind = local->kind;
     a.dim = local->dim;
+  }
+  if ((n == 512 || n == 1024) && C == 3) {
+    const cudaError_t e = long_r2c_launch<T>(a, n, local, st);
+    if (e != cudaErrorNotSupported) return e;
   }
   if ((n == 64 || n == 128 || n == 256) && (C == 3 || C == 6)) {
     // compile-time tiles: W = 12 columns (6 for n = 256), R = 2 W / C rows
@@ -1528,6 +1601,10 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
     if ((epi == kEpiResid || epi == kEpiRhs) && !a.contig) return cudaErrorInvalidValue;
     if (epi == kEpiResid && (sizeof(T) != 8 || !upd->rout)) return cudaErrorInvalidValue;
     if (epi == kEpiRhs && !upd->rhs) return cudaErrorInvalidValue;
+  }
+  if ((n == 512 || n == 1024) && C == 3) {
+    const cudaError_t e = long_c2r_launch<T>(a, n, epi, nb_out, st);
+    if (e != cudaErrorNotSupported) return e;
   }
   if ((n == 64 || n == 128 || n == 256) && (C == 3 || C == 6)) {
     const int wct = n <= 128 ? 12 : 6;
@@ -1724,8 +1801,13 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     if (al16(in) && al16(out) && (a.pitch * cs) % 16 == 0 &&
         cols_tma_shape(sizeof(T) == 8 ? F64 : F32, n, mode == 2 ? C : 1, &Wp, &sp, &nbuf,
                        mode == 2 && a.mn == nullptr, tune)) {
-      int nbox = n <= 256 ? n : 256;  // rows per box: largest divisor of n up to 256
-      while (n % nbox != 0) --nbox;
+      // rows per box: the largest divisor of n up to 256 whose boxes start
+      // on 128-byte boundaries of the tile (a tensor copy's shared-memory
+      // address must be 128-byte aligned: n = 700 in FP64 takes 140-row
+      // boxes, not 175)
+      int nbox = n <= 256 ? n : 256;
+      while (nbox > 1 && (n % nbox != 0 || (nbox < n && (nbox * (size_t)Wp * cs) % 128 != 0)))
+        --nbox;
       CUtensorMap tin, tout;
       if (nbox >= 8 &&
           make_cols_map(&tin, in, sizeof(T) == 8, inner, a.pitch, n, outer, Wp, nbox) &&

@@ -108,7 +108,10 @@ def test_r2c_strided_tensor():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(128, 128), (64, 32, 48), (96, 100)])
+# (375, 40), (700, 24): column passes whose row count has no divisor up to
+# 256 with 128-byte-aligned tensor-copy boxes (375) or only a smaller one
+# (700: 140-row boxes rather than 175)
+@pytest.mark.parametrize("shape", [(128, 128), (64, 32, 48), (96, 100), (375, 40), (700, 24)])
 def test_fp32_transform(shape):
     rng = np.random.default_rng(2)
     a = rng.uniform(-1, 1, size=shape)
