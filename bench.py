@@ -1056,6 +1056,50 @@ def run_kernels(args, rank):
     print(json.dumps({"workload": "kernels", "calls": calls}), flush=True)
 
 
+def run_passes2d(args, rank):
+    """Per-pass device times of one basic-scheme step on n x n 2D grids
+    (filtered, 3 load cases, 30% inclusions), n in --passes2d-n, FP64 and
+    FP32: ms per pass (CUDA events around each pass, mean of --steps steps
+    after --warmup) and the fraction of measured HBM bandwidth from the
+    algorithmic bytes 2sp + 1 (r2c with the phase map), 2sp (Green pass), 3sp
+    (c2r with the update) per voxel and load case."""
+    import numpy as np
+    import torch
+
+    import janus_b200.material.elastic.linear.isotropic as material
+    from janus_b200 import autotune
+    from janus_b200 import operators as ops
+    from janus_b200.green import filtered
+    from janus_b200.solvers import BasicScheme
+
+    peak, _ = measured_peak()
+    for n in [int(v) for v in args.passes2d_n.split(",")]:
+        for dt in (torch.float64, torch.float32):
+            rng = np.random.default_rng(0)
+            phase = (rng.random((n, n)) < 0.3).astype(np.uint8)
+            mat0 = material.create(50.5, 0.3, 2)
+            tens = [ops.isotropic_4(2 * (material.create(g, nu, 2).k - mat0.k), 2 * (g - 50.5), 2)
+                    for g, nu in ((1.0, 0.3), (100.0, 0.2))]
+            loc = ops.BlockDiagonalOperator2D.from_phases(phase, tens, dtype=dt)
+            g = filtered(mat0.green_operator(), (n, n), 1.0, dtype=dt)
+            sol = BasicScheme(g, loc, 3)
+            sol.set_load(np.eye(3))
+            eps = sol.new_field()
+            res = torch.zeros(3, dtype=torch.float64, device=eps.device)
+            t = autotune._time_passes(sol, eps, res, max(args.steps, 5), max(args.warmup, 3))
+            p = 8 if dt == torch.float64 else 4
+            vox = 3 * n * n
+            alg = {"rows_r2c_local": (2 * 3 * p + 1) * vox, "cols_green_axis0": 2 * 3 * p * vox,
+                   "rows_c2r_update": 3 * 3 * p * vox}
+            out = {k: {"ms": round(v, 4),
+                       "frac": round(alg[k] / (v * 1e-3) / 1e9 / peak, 3) if k in alg else None}
+                   for k, v in t.items()}
+            print(json.dumps({"workload": "passes2d", "n": n, "dtype": str(dt)[6:],
+                              "passes": out}), flush=True)
+            del sol, eps, g, loc
+            torch.cuda.empty_cache()
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -1105,9 +1149,12 @@ def main(argv=None):
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the column-schedule autotuner (built-in rules)")
     ap.add_argument("--workload", default="spheres3d",
-                    choices=["spheres3d", "batch2d", "voronoi", "gradients", "kernels"],
+                    choices=["spheres3d", "batch2d", "voronoi", "gradients", "kernels",
+                             "passes2d"],
                     help="spheres3d: the headline step; batch2d: batched 2D cells; "
                          "voronoi: mixed vs FP64 time-to-solution on a 3D Voronoi cell")
+    ap.add_argument("--passes2d-n", default="256,512,768,1024",
+                    help="grid sizes of the passes2d workload")
     ap.add_argument("--voronoi-n", type=int, default=256)
     ap.add_argument("--grad-n", type=int, default=128)
     ap.add_argument("--grad-batch", type=int, default=8)
@@ -1170,6 +1217,10 @@ def main(argv=None):
     if args.workload == "kernels":
         if rank == 0:
             run_kernels(args, rank)
+        return
+    if args.workload == "passes2d":
+        if rank == 0:
+            run_passes2d(args, rank)
         return
 
     dist = None

@@ -160,9 +160,10 @@ int jb_green_apply_noalloc(int dim, const int64_t *shape, double h, double g,
  * compile-time tiles allowed}; widths in complex columns (the Green one a
  * multiple of s), input tiles 2 or 3, 0 = built-in rule; a Green
  * compile-time value of 2 transforms the Green tiles in place (24 columns at
- * n = 128, 12 at n = 256, no partner tile), 3 takes the Green pass whose
- * middle radix-4 stage and contraction run in registers (n0 = 32, 64, 128;
- * also the built-in rule there).  A width whose tiles do not fit the
+ * n = 128, 12 at n = 256, no partner tile), 3 takes the register-tile Green
+ * pass (n0 = 32 ... 1024, a power of two: the axis-0 transforms and the
+ * contraction in registers between shared-memory exchanges; the built-in
+ * rule except 3D n0 = 256 and 3D FP32 n0 = 128 on the fly).  A width whose tiles do not fit the
  * shared-memory budget is narrowed.  An optional 7th value selects the Green
  * contraction: 0 built-in rule (the table for the filtered operator, on the
  * fly for the truncated and finite-difference ones), 1 the table of

@@ -763,7 +763,7 @@ int jb_green_set_tuning(jb_green* G, const int* v, int count) {
     if (k != 0 && k != 2 && k != 3) return fail(JB_EINVAL, "input tiles must be 0, 2 or 3");
   if (v[5] < 0 || v[5] > 3)
     return fail(JB_EINVAL,
-                "Green compile-time value must be 0, 1, 2 (in place) or 3 (register radix-4)");
+                "Green compile-time value must be 0, 1, 2 (in place) or 3 (register tiles)");
   G->tune_plain.w = v[0];
   G->tune_plain.nbuf = v[1];
   G->tune_plain.ct = v[2] != 0;

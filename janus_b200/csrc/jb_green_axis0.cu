@@ -520,7 +520,7 @@ cudaError_t axis0_t(const AxisData& ax0, int64_t L, int64_t inner, int64_t pitch
                     const void* in, void* out, int C, int dim, const GreenDeviceTables& gt,
                     int64_t m_last, cudaStream_t st) {
   const int n0 = ax0.plan.n;
-  if (!green_axis0_r4_supported(n0, C, dim)) return cudaErrorNotSupported;
+  if (!green_axis0_regs_supported(n0, C, dim)) return cudaErrorNotSupported;
   if (L < 1 || L > 65535 || inner < 1 || (inner % C) != 0 || pitch < inner)
     return cudaErrorInvalidValue;
   const size_t cs = sizeof(cx<T>);
@@ -557,12 +557,12 @@ cudaError_t axis0_t(const AxisData& ax0, int64_t L, int64_t inner, int64_t pitch
 
 }  // namespace
 
-bool green_axis0_r4_supported(int n0, int C, int dim) {
+bool green_axis0_regs_supported(int n0, int C, int dim) {
   return (n0 == 32 || n0 == 64 || n0 == 128 || n0 == 256 || n0 == 512 || n0 == 1024) &&
          ((dim == 3 && C == 6) || (dim == 2 && C == 3));
 }
 
-cudaError_t launch_green_axis0_r4(int dtype, const AxisData& ax0, int64_t L, int64_t inner,
+cudaError_t launch_green_axis0_regs(int dtype, const AxisData& ax0, int64_t L, int64_t inner,
                                   int64_t pitch, const void* in, void* out, int C, int dim,
                                   const GreenDeviceTables& gt, int64_t m_last,
                                   cudaStream_t st) {

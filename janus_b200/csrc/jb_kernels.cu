@@ -1763,11 +1763,11 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     // the fly at 3D n = 128: 0.191 vs 0.210 ms at 128^3 x 6)
     const bool rule_reg = rule && !(dim == 3 && n == 256) &&
                           !(dim == 3 && n == 128 && sizeof(T) == 4 && a.mn == nullptr);
-    if (mode == 2 && gt && green_axis0_r4_supported(n, C, dim) &&
+    if (mode == 2 && gt && green_axis0_regs_supported(n, C, dim) &&
         ((tune && tune->ct == 3) || rule_reg)) {
       GreenDeviceTables g2 = *gt;
       g2.mn = a.mn;
-      const cudaError_t e = launch_green_axis0_r4(sizeof(T) == 8 ? F64 : F32, ax, outer, inner,
+      const cudaError_t e = launch_green_axis0_regs(sizeof(T) == 8 ? F64 : F32, ax, outer, inner,
                                                   a.pitch, in, out, C, dim, g2, m_last, st);
       if (e != cudaErrorNotSupported) return e;
     }

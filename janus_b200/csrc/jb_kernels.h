@@ -137,9 +137,8 @@ cudaError_t launch_rows_c2r(int dtype, const AxisData& ax, int C, int L, const v
 // complex columns (a multiple of the coefficient size for the Green pass),
 // rotating input tiles (2 or 3), and whether compile-time FFT tiles may be
 // used where they exist (0 no, 1 yes, 2 Green tiles transformed in place:
-// 24 columns at n = 128, 12 at n = 256, no partner tile; 3 the Green pass
-// with its middle radix-4 stage in registers, n = 32, 64, 128).  Chosen per
-// operator by the autotuner.
+// 24 columns at n = 128, 12 at n = 256, no partner tile; 3 the register-tile
+// Green pass, n = 32 ... 1024).  Chosen per operator by the autotuner.
 struct ColsTuning {
   int w = 0;
   int nbuf = 0;
@@ -155,12 +154,12 @@ cudaError_t launch_cols(int dtype, const AxisData& ax, int mode, int64_t outer,
                         const GreenDeviceTables* gt, int64_t n1, int64_t m_last,
                         cudaStream_t st, const ColsTuning* tune = nullptr,
                         int64_t pitch = 0);
-// Axis-0 Green pass for n0 = 32, 64, 128 with the middle radix-4 stage and
-// the contraction in registers (jb_green_axis0.cu): in/out complex
+// Axis-0 Green pass for n0 = 32 ... 1024 (powers of two) as register tiles
+// (five phases up to 256, seven at 512 and 1024; jb_green_axis0.cu): in/out complex
 // [L][n0][pitch] (the first `inner` = F * C of each row), in place allowed;
 // gt.mn, when set, is the operator table of launch_green_table.
-bool green_axis0_r4_supported(int n0, int C, int dim);
-cudaError_t launch_green_axis0_r4(int dtype, const AxisData& ax0, int64_t L, int64_t inner,
+bool green_axis0_regs_supported(int n0, int C, int dim);
+cudaError_t launch_green_axis0_regs(int dtype, const AxisData& ax0, int64_t L, int64_t inner,
                                   int64_t pitch, const void* in, void* out, int C, int dim,
                                   const GreenDeviceTables& gt, int64_t m_last,
                                   cudaStream_t st);

@@ -20,7 +20,7 @@ def test_candidates_respect_the_coefficient_size():
         assert {w for w, _, ct in sized if ct != 2} == {s, 2 * s, 3 * s}
         # the in-place variants: 24 columns (n = 128) and 12 (n = 256)
         assert sorted(c for c in green if c[2] == 2) == [(12, 2, 2), (24, 2, 2)]
-        # the register radix-4 pass has a fixed tile (width and tiles 0)
+        # the register-tile pass has a fixed tile (width and tiles 0)
         assert [c for c in green if c[2] == 3] == [(0, 0, 3)]
         if dim == 2:
             assert plain == []   # 2D has no plain column pass
