@@ -108,6 +108,46 @@ template <int DIR, typename C> struct Dft<5, DIR, C> {
   }
 };
 
+// 6 = 2 x 3 and 12 = 4 x 3 by the prime-factor (Good-Thomas) mapping, which
+// needs no twiddles for coprime factors P, Q: input n = (Q p + P q) mod PQ,
+// a Q-point DFT over q for each p, a P-point DFT over p for each output
+// residue, output k = the CRT index with k = k1 mod P, k = k2 mod Q.
+template <int P, int Q, int DIR, typename C>
+__device__ __forceinline__ void dft_pfa(C* v, const int (&kmap)[P][Q]) {
+  C a[P][Q];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) a[p][q] = v[(Q * p + P * q) % (P * Q)];
+    Dft<Q, DIR, C>::run(a[p]);
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    C g[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) g[p] = a[p][q];
+    Dft<P, DIR, C>::run(g);
+#pragma unroll
+    for (int p = 0; p < P; ++p) v[kmap[p][q]] = g[p];
+  }
+}
+
+template <int DIR, typename C> struct Dft<6, DIR, C> {
+  // k = (3 k1 + 4 k2) mod 6
+  __device__ __forceinline__ static void run(C* v) {
+    constexpr int km[2][3] = {{0, 4, 2}, {3, 1, 5}};
+    dft_pfa<2, 3, DIR>(v, km);
+  }
+};
+
+template <int DIR, typename C> struct Dft<12, DIR, C> {
+  // k = (9 k1 + 4 k2) mod 12
+  __device__ __forceinline__ static void run(C* v) {
+    constexpr int km[4][3] = {{0, 4, 8}, {9, 1, 5}, {6, 10, 2}, {3, 7, 11}};
+    dft_pfa<4, 3, DIR>(v, km);
+  }
+};
+
 template <int DIR, typename C> struct Dft<8, DIR, C> {
   __device__ __forceinline__ static void run(C* v) {
     using T = decltype(v[0].x);

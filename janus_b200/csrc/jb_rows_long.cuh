@@ -1,4 +1,4 @@
-// Row passes along long contiguous axes (n = 512, 1024) of three-component
+// Row passes along long contiguous axes (n = 512, 768, 1024) of three-component
 // 2D fields: persistent, pipelined kernels.  Included by jb_kernels.cu inside
 // its kernel namespace (uses RowsArgs, the local operator and block_sum).
 //
@@ -10,8 +10,9 @@
 //    H = n/2 points, unpacked into the half spectrum X_c[0..H] with one
 //    twiddle per coefficient pair (k, H-k) (r2c), and packed the other way
 //    before the inverse (c2r);
-//  * H = N1 * 64 points as three register phases (N1-, 8- and 8-point
-//    transforms, n' = j + 64 m, j = ja + 8 jb, k = k1 + N1 (kb + 8 ka)) on a
+//  * H = N1 * 64 points (N1 = 4, 6, 8) as three register phases (N1-, 8-
+//    and 8-point transforms, n' = j + 64 m, j = ja + 8 jb, k = k1 + N1 (kb +
+//    8 ka)) on a
 //    tile whose rows k1 are PK = 193 (FP64) / 194 (FP32) complex apart, so
 //    the lanes of every phase (k1 fastest) hit distinct banks;
 //  * one CTA of 192 threads walks the rows (l, r) = t, t + grid, ...; loads
@@ -27,7 +28,7 @@ template <typename T, int N> struct LongRow {
   static constexpr int THREADS = 192;
   static constexpr int P23 = N1 * 24;   // lanes of phases 2 and 3
   static constexpr int PAIRS = 3 * N1 * (H / (2 * N1) + 1);  // pair jobs (k <= H/2)
-  static constexpr int MINB = sizeof(T) == 8 ? (N == 1024 ? 2 : 4) : (N == 1024 ? 4 : 5);
+  static constexpr int MINB = sizeof(T) == 8 ? (N == 512 ? 4 : 2) : (N == 512 ? 5 : 4);
   static constexpr size_t RAWB = ((size_t)N * 3 * sizeof(T) + 127) / 128 * 128;
 };
 
@@ -70,7 +71,7 @@ __host__ __device__ inline LongC2rLayout long_c2r_layout(size_t cs, int n) {
 
 // tile position of natural coefficient k (component c) after phase 3
 template <typename K> __device__ __forceinline__ int lr_zpos(int k, int c) {
-  const int k1 = k & (K::N1 - 1), k2 = k / K::N1;
+  const int k1 = k % K::N1, k2 = k / K::N1;
   return k1 * K::PK + ((k2 >> 3) + 8 * (k2 & 7)) * 3 + c;
 }
 
@@ -81,8 +82,9 @@ template <typename K> __device__ __forceinline__ int lr_ipos(int k, int c) {
 
 // w_n^i, 0 <= i < n, from the half table
 template <int N, typename C> __device__ __forceinline__ C lr_tw(const C* tw, int i) {
-  const C w = tw[i & (N / 2 - 1)];
-  return i < N / 2 ? w : mkc(-w.x, -w.y);
+  const bool hi = i >= N / 2;
+  const C w = tw[hi ? i - N / 2 : i];
+  return hi ? mkc(-w.x, -w.y) : w;
 }
 
 // phases 1-3 of the H-point transform of the three columns in tile z.
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(LongRow<T, N>::THREADS, LongRow<T, N>::MINB)
       const int k = k1 + N1 * k2;
       if (k > H / 2) continue;
       const C Z = tile[lr_zpos<K>(k, c)];
-      const C Zh = tile[lr_zpos<K>((H - k) & (H - 1), c)];
+      const C Zh = tile[lr_zpos<K>(k == 0 ? 0 : H - k, c)];
       // A = (Z + conj Zh)/2, P = w^k (Z - conj Zh):
       // X[k] = A - (i/2) P, X[H-k] = conj A - (i/2) conj P
       const T ax = T(0.5) * (Z.x + Zh.x), ay = T(0.5) * (Z.y - Zh.y);
