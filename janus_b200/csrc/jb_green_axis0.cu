@@ -30,9 +30,9 @@
 // 85 registers in FP64 (128 where both transforms hold 16 values), so that
 // three CTAs of 256 threads share an SM, and 51 in FP32 (five CTAs).
 //
-// n0 = 512, 768, 1024: seven-phase tiles, the same scheme with the N2-point
-// transform split once more (512 = 8 8 8, 768 = 12 8 8, 1024 = 16 8 8): P1
-// (the 12-point transform by the prime-factor mapping 4 x 3), then an
+// n0 = 192, 384, 512, 768, 1024: seven-phase tiles, the same scheme with the
+// N2-point transform split once more (N1 8 8 with N1 = 3, 6, 8, 12, 16): P1
+// (6 and 12 points by the prime-factor mappings 2 x 3 and 4 x 3), then an
 // 8-point transform over the high part of j with its twiddles, an 8-point
 // transform over the low part, the contraction, and the mirror images; the
 // middle phases loop over more jobs than the block has lanes.
@@ -324,7 +324,7 @@ cudaError_t axis0_r8_go(const Axis0Args<T>& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// ---- seven-phase tiles (n0 = 512, 768, 1024) ----
+// ---- seven-phase tiles (n0 = 192, 384, 512, 768, 1024) ----
 
 // n0 = N1 A B: n = j + M m (M = A B), k = k1 + N1 k2; the M-point transform
 // over j = ja + A jb is split again, k2 = kb + B ka:
@@ -342,7 +342,10 @@ cudaError_t axis0_r8_go(const Axis0Args<T>& a, cudaStream_t st) {
 template <int N0> struct R16Shape;
 template <> struct R16Shape<512> { static constexpr int N1 = 8, A = 8, B = 8; };
 template <> struct R16Shape<1024> { static constexpr int N1 = 16, A = 8, B = 8; };
-// 768 = 12 * 64: the first phase a 12-point (4 x 3 prime-factor) transform
+// 192, 384, 768 = 3, 6, 12 times 64: a 3-point first phase, or a 6- or
+// 12-point one (2 x 3, 4 x 3 prime-factor transforms)
+template <> struct R16Shape<192> { static constexpr int N1 = 3, A = 8, B = 8; };
+template <> struct R16Shape<384> { static constexpr int N1 = 6, A = 8, B = 8; };
 template <> struct R16Shape<768> { static constexpr int N1 = 12, A = 8, B = 8; };
 
 template <typename T, int DIM, int N0> struct R16Tile {
@@ -508,6 +511,8 @@ cudaError_t axis0_n(const Axis0Args<T>& a, int n0, cudaStream_t st) {
     case 64: return axis0_r8_go<T, DIM, 64, TAB>(a, st);
     case 128: return axis0_r8_go<T, DIM, 128, TAB>(a, st);
     case 256: return axis0_r8_go<T, DIM, 256, TAB>(a, st);
+    case 192: return axis0_r16_go<T, DIM, 192, TAB>(a, st);
+    case 384: return axis0_r16_go<T, DIM, 384, TAB>(a, st);
     case 512: return axis0_r16_go<T, DIM, 512, TAB>(a, st);
     case 768: return axis0_r16_go<T, DIM, 768, TAB>(a, st);
     default: return axis0_r16_go<T, DIM, 1024, TAB>(a, st);
@@ -562,8 +567,8 @@ cudaError_t axis0_t(const AxisData& ax0, int64_t L, int64_t inner, int64_t pitch
 }  // namespace
 
 bool green_axis0_regs_supported(int n0, int C, int dim) {
-  return (n0 == 32 || n0 == 64 || n0 == 128 || n0 == 256 || n0 == 512 || n0 == 768 ||
-          n0 == 1024) &&
+  return (n0 == 32 || n0 == 64 || n0 == 128 || n0 == 192 || n0 == 256 || n0 == 384 ||
+          n0 == 512 || n0 == 768 || n0 == 1024) &&
          ((dim == 3 && C == 6) || (dim == 2 && C == 3));
 }
 

@@ -1121,7 +1121,7 @@ __global__ void reduce_rows_kernel(const double* partials, int nb, double* out, 
   }
 }
 
-// long contiguous rows (n = 512, 768, 1024) of 2D fields
+// long contiguous rows (n = 384, 512, 768, 1024) of 2D fields
 #include "jb_rows_long.cuh"
 
 std::mutex g_attr_mu;
@@ -1415,7 +1415,7 @@ cudaError_t c2r_ct_dispatch(int C, int epi, const RowsArgs<T>& a, dim3 grid, siz
   return cudaErrorNotSupported;
 }
 
-// Long contiguous rows (n = 512, 768, 1024, three components): the persistent
+// Long contiguous rows (n = 384, 512, 768, 1024, three components): the persistent
 // kernels of jb_rows_long.cuh when every row satisfies their bulk-copy rules
 // (16-byte aligned bases and pitches, a spectral row of a multiple of 16
 // bytes, a tail of the spectral row of 3 or 4 complex); cudaErrorNotSupported
@@ -1444,6 +1444,8 @@ cudaError_t long_r2c_launch(const RowsArgs<T>& a, int n, const LocalDesc* local,
                               : go(&rows_long_r2c_kernel<T, 1024, false>, TH);
   if (n == 768) return local ? go(&rows_long_r2c_kernel<T, 768, true>, TH)
                              : go(&rows_long_r2c_kernel<T, 768, false>, TH);
+  if (n == 384) return local ? go(&rows_long_r2c_kernel<T, 384, true>, TH)
+                             : go(&rows_long_r2c_kernel<T, 384, false>, TH);
   return local ? go(&rows_long_r2c_kernel<T, 512, true>, TH)
                : go(&rows_long_r2c_kernel<T, 512, false>, TH);
 }
@@ -1481,6 +1483,13 @@ cudaError_t long_c2r_launch(const RowsArgs<T>& a, int n, int epi, int* nb_out, c
       case kEpiUpdate: return go(&rows_long_c2r_kernel<T, 768, kEpiUpdate>);
       case kEpiRhs: return go(&rows_long_c2r_kernel<T, 768, kEpiRhs>);
       default: return go(&rows_long_c2r_kernel<T, 768, kEpiPlain>);
+    }
+  }
+  if (n == 384) {
+    switch (epi) {
+      case kEpiUpdate: return go(&rows_long_c2r_kernel<T, 384, kEpiUpdate>);
+      case kEpiRhs: return go(&rows_long_c2r_kernel<T, 384, kEpiRhs>);
+      default: return go(&rows_long_c2r_kernel<T, 384, kEpiPlain>);
     }
   }
   switch (epi) {
@@ -1528,7 +1537,7 @@ cudaError_t rows_r2c_t(const AxisData& ax, int C, int L, const void* x, const Re
     a.kind = local->kind;
     a.dim = local->dim;
   }
-  if ((n == 512 || n == 768 || n == 1024) && C == 3) {
+  if ((n == 384 || n == 512 || n == 768 || n == 1024) && C == 3) {
     const cudaError_t e = long_r2c_launch<T>(a, n, local, st);
     if (e != cudaErrorNotSupported) return e;
   }
@@ -1611,7 +1620,7 @@ cudaError_t rows_c2r_t(const AxisData& ax, int C, int L, const void* in, void* y
     if (epi == kEpiResid && (sizeof(T) != 8 || !upd->rout)) return cudaErrorInvalidValue;
     if (epi == kEpiRhs && !upd->rhs) return cudaErrorInvalidValue;
   }
-  if ((n == 512 || n == 768 || n == 1024) && C == 3) {
+  if ((n == 384 || n == 512 || n == 768 || n == 1024) && C == 3) {
     const cudaError_t e = long_c2r_launch<T>(a, n, epi, nb_out, st);
     if (e != cudaErrorNotSupported) return e;
   }

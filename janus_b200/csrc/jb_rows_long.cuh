@@ -1,4 +1,4 @@
-// Row passes along long contiguous axes (n = 512, 768, 1024) of three-component
+// Row passes along long contiguous axes (n = 384, 512, 768, 1024) of three-component
 // 2D fields: persistent, pipelined kernels.  Included by jb_kernels.cu inside
 // its kernel namespace (uses RowsArgs, the local operator and block_sum).
 //
@@ -10,7 +10,7 @@
 //    H = n/2 points, unpacked into the half spectrum X_c[0..H] with one
 //    twiddle per coefficient pair (k, H-k) (r2c), and packed the other way
 //    before the inverse (c2r);
-//  * H = N1 * 64 points (N1 = 4, 6, 8) as three register phases (N1-, 8-
+//  * H = N1 * 64 points (N1 = 3, 4, 6, 8) as three register phases (N1-, 8-
 //    and 8-point transforms, n' = j + 64 m, j = ja + 8 jb, k = k1 + N1 (kb +
 //    8 ka)) on a
 //    tile whose rows k1 are PK = 193 (FP64) / 194 (FP32) complex apart, so
@@ -28,7 +28,7 @@ template <typename T, int N> struct LongRow {
   static constexpr int THREADS = 192;
   static constexpr int P23 = N1 * 24;   // lanes of phases 2 and 3
   static constexpr int PAIRS = 3 * N1 * (H / (2 * N1) + 1);  // pair jobs (k <= H/2)
-  static constexpr int MINB = sizeof(T) == 8 ? (N == 512 ? 4 : 2) : (N == 512 ? 5 : 4);
+  static constexpr int MINB = sizeof(T) == 8 ? (N <= 512 ? 4 : 2) : (N <= 512 ? 5 : 4);
   static constexpr size_t RAWB = ((size_t)N * 3 * sizeof(T) + 127) / 128 * 128;
 };
 

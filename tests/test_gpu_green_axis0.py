@@ -1,6 +1,6 @@
 """The axis-0 Green pass whose transforms and contraction run in registers
-(five-phase tiles for n0 = 32 ... 256, seven-phase tiles for 512, 768 and
-1024, 768 with a 12-point first phase),
+(five-phase tiles for n0 = 32 ... 256, seven-phase tiles for 192, 384, 512,
+768 and 1024, with 3-, 6-, 8-, 12- and 16-point first phases),
 against the oracle and against the shared-memory column kernel, for the
 three discretisations of janus/green.pyx (truncated 393-580, filtered
 583-973 through the generic c_apply 185-216 / 356-390, finite differences
@@ -23,9 +23,9 @@ NU = 0.3
 FACTORY = {"truncated": truncated, "filtered": filtered, "willot": willot2015}
 # n0 from 32 to 1024 (five-phase tiles up to 256, seven-phase above); ragged
 # coefficient counts in the last tile
-SHAPES = [(128, 6, 10), (128, 5, 4), (64, 5, 8), (32, 9, 6), (256, 3, 6), (512, 2, 4),
-          (768, 2, 4), (1024, 1, 6), (128, 18), (64, 7), (32, 33), (256, 10), (512, 6),
-          (768, 10), (1024, 14)]
+SHAPES = [(128, 6, 10), (128, 5, 4), (64, 5, 8), (32, 9, 6), (192, 3, 6), (256, 3, 6),
+          (384, 2, 6), (512, 2, 4), (768, 2, 4), (1024, 1, 6), (128, 18), (64, 7), (32, 33),
+          (192, 12), (256, 10), (384, 9), (512, 6), (768, 10), (1024, 14)]
 # register-tile Green pass (compile-time value 3), the contraction by the
 # built-in rule
 R4 = [0, 0, 1, 0, 0, 3, 0]

@@ -1,4 +1,4 @@
-"""Row passes along 512-, 768- and 1024-point axes (the persistent long-row
+"""Row passes along 384-, 512-, 768- and 1024-point axes (the persistent long-row
 kernels for three-component fields, the runtime-plan row kernels for the FFT
 objects): the FFT objects against numpy's FFT with the reference's tolerance
 model (tests/test_fft.py:9-80 of the reference), and the basic scheme on
@@ -55,7 +55,7 @@ def _phase(shape, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(32, 1024), (48, 512), (40, 768)])
+@pytest.mark.parametrize("shape", [(32, 1024), (48, 512), (40, 768), (24, 384)])
 @pytest.mark.parametrize("variant", ["filtered", "truncated"])
 def test_long_rows_basic_scheme_per_iterate(shape, variant):
     """FP64: every iterate within 1e-12 of the oracle; FP32 (rows of width 3)
@@ -92,7 +92,7 @@ def test_long_rows_mixed_scheme():
 # Rows x load cases well above twice the persistent grid of the long-row
 # kernels, so every CTA walks several rows through both buffers; ragged row
 # counts, so the CTAs' row runs cross load cases at different points.
-MANY_ROWS = [(512, 1024), (700, 512), (37, 1024), (300, 768)]
+MANY_ROWS = [(512, 1024), (700, 512), (37, 1024), (300, 768), (1100, 384)]
 
 
 def _per_load(phase, E, iters, variant, dtype, tol, loc_fn, oracle_fn):
@@ -180,7 +180,8 @@ def test_long_rows_matrix_phases():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(300, 1024), (45, 512), (96, 768), (768, 768)])
+@pytest.mark.parametrize("shape", [(300, 1024), (45, 512), (96, 768), (768, 768), (384, 384),
+                                   (192, 384)])
 @pytest.mark.parametrize("variant", ["filtered", "truncated"])
 def test_long_rows_green_apply(shape, variant):
     """The plain r2c / c2r passes (no local operator, no epilogue) through
