@@ -1776,11 +1776,13 @@ cudaError_t cols_t(const AxisData& ax, int mode, int64_t outer, int64_t inner, c
     // 256: -17%, FP32 256: -8%, FP32 128: -5%, FP64 128: equal)
     const bool rule = !tune || (tune->w == 0 && tune->nbuf == 0 && tune->ct == 1);
     // the register-tile Green pass (n = 32 ... 1024): tuning value ct = 3;
-    // the built-in rule takes it except where the in-place tiles measured
-    // faster on B200 (3D n = 256: 1.22 vs 1.41 ms FP64 at 256^3 x 2; FP32 on
-    // the fly at 3D n = 128: 0.191 vs 0.210 ms at 128^3 x 6)
+    // the built-in rule takes it except where the in-place or column tiles
+    // measured faster on B200 (3D n = 256: 1.22 vs 1.41 ms FP64 at 256^3 x 2;
+    // FP32 on the fly at 3D n = 128: 0.191 vs 0.210 ms at 128^3 x 6; FP32 at
+    // 3D n = 192: 0.50 vs 0.57 ms filtered at 192^3 x 2)
     const bool rule_reg = rule && !(dim == 3 && n == 256) &&
-                          !(dim == 3 && n == 128 && sizeof(T) == 4 && a.mn == nullptr);
+                          !(dim == 3 && n == 128 && sizeof(T) == 4 && a.mn == nullptr) &&
+                          !(dim == 3 && n == 192 && sizeof(T) == 4);
     if (mode == 2 && gt && green_axis0_regs_supported(n, C, dim) &&
         ((tune && tune->ct == 3) || rule_reg)) {
       GreenDeviceTables g2 = *gt;
