@@ -1,6 +1,7 @@
-// Row passes along long contiguous axes (n = 384, 512, 768, 1024) of three-component
-// 2D fields: persistent, pipelined kernels.  Included by jb_kernels.cu inside
-// its kernel namespace (uses RowsArgs, the local operator and block_sum).
+// Row passes along long contiguous axes (n = 384, 512, 768, 1024) of
+// three-component 2D fields: persistent, pipelined kernels.  Included by
+// jb_kernels.cu inside its kernel namespace (uses RowsArgs, the local
+// operator and block_sum).
 //
 // The general row kernels pair two real columns of the tile into one complex
 // column and transform n points; with one 1024-point FP64 row per CTA (three
@@ -12,9 +13,9 @@
 //    before the inverse (c2r);
 //  * H = N1 * 64 points (N1 = 3, 4, 6, 8) as three register phases (N1-, 8-
 //    and 8-point transforms, n' = j + 64 m, j = ja + 8 jb, k = k1 + N1 (kb +
-//    8 ka)) on a
-//    tile whose rows k1 are PK = 193 (FP64) / 194 (FP32) complex apart, so
-//    the lanes of every phase (k1 fastest) hit distinct banks;
+//    8 ka)) on a tile whose rows k1 are PK = 193 (FP64) / 194 (FP32)
+//    complex apart, so the lanes of phases 2 and 3 (k1 fastest) meet at most
+//    two-way bank conflicts;
 //  * one CTA of 192 threads walks the rows (l, r) = t, t + grid, ...; loads
 //    and stores are bulk copies issued by thread 0, one row or more ahead.
 // Half twiddle table: w_n^i for i < n/2 in shared memory, w_n^(i + n/2) =
