@@ -155,6 +155,13 @@ def test_timed_out_copy_wait_is_reported():
         loc, green = _problem(phase, [(1.0, 0.3), (10.0, 0.3)], 5.5, 0.3)
         with pytest.raises(RuntimeError, match="bounded wait"):
             BasicScheme(green, loc).run(np.eye(6)[:1], 5)
+        # a 2D cell on 1024-point rows: the persistent long-row kernels give
+        # up at their first wait and let the other row buffers' copies land
+        # (three load cases, so every CTA has rows queued behind the first)
+        phase2 = (rng.random((300, 1024)) < 0.3).astype(np.uint8)
+        loc2, green2 = _problem(phase2, [(1.0, 0.3), (10.0, 0.3)], 5.5, 0.3, "filtered")
+        with pytest.raises(RuntimeError, match="bounded wait"):
+            BasicScheme(green2, loc2, nload=3).run(np.eye(3), 3)
     finally:
         _lib.set_wait_limit()
         _lib.device_status()
