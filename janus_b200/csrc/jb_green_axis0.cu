@@ -362,8 +362,11 @@ template <typename T, int DIM, int N0> struct R16Tile {
   static constexpr size_t SMEM = (size_t)N1 * PK * sizeof(cx<T>);
   // 24 warps per SM in FP64 (at most 85 registers: the 1024-point tile
   // spills about 200 bytes there and still measured faster than at 12 warps
-  // without spills), 32 in FP32
-  static constexpr int MINB = (sizeof(T) == 8 ? 24 : 32) * 32 / THREADS;
+  // without spills); in FP32 24, and 36 for the 1024-point tile (56
+  // registers, no spills: 1024^2 x 3 Green pass 0.0481 -> 0.0451 ms, while
+  // the 768-point tile measured 0.0310 -> 0.0350 ms at that cap)
+  static constexpr int MINB =
+      (sizeof(T) == 8 ? 24 : (N0 == 1024 ? 36 : 24)) * 32 / THREADS;
 };
 
 template <typename T, int DIM, int N0, bool TAB>
